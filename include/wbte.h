@@ -1,0 +1,213 @@
+/*
+ * wbte.h -- C ABI of libwbte, the sm_100a (B200) implementation of the
+ * batched threshold-decryption path of the btx / weighted_btx / pfe /
+ * weighted_pfe crates over BLS12-381.
+ *
+ * The reference crates reach all of their heavy arithmetic through blst's C
+ * ABI (blst 0.3.17 via blstrs 0.7.1).  Each entry point below replaces one of
+ * those call sites, or one hot loop of the crate that is built from them, and
+ * keeps blst's memory layout so that Rust wrappers can pass the same buffers:
+ *
+ *   Fp     48 bytes: 6 little-endian 64-bit limbs, Montgomery form, R = 2^384
+ *   G1     96 bytes: affine (x, y)                    (blst_p1_affine)
+ *   G2    192 bytes: affine (x.c0, x.c1, y.c0, y.c1)  (blst_p2_affine)
+ *   GT    576 bytes: Fp12, c0.c0.c0 first             (blst_fp12)
+ *   Fr     32 bytes: canonical little-endian integer  (Scalar::to_bytes_le,
+ *                    the scalar format of blst_p{1,2}s_mult_pippenger)
+ *   The point at infinity is all zero bytes (blst's affine convention).
+ *
+ * Buffers.  Every data pointer may be host memory or device memory of the
+ * context's GPU; the library detects which.  Host inputs are copied in, host
+ * outputs are copied out before the call returns (the call is then
+ * synchronous).  When every data pointer is device memory the call only
+ * enqueues work on the context's stream and returns; synchronise with
+ * wbte_ctx_synchronize().  Arrays of indices and offsets marked "host" must
+ * be host memory.  Callers own all buffers; nothing is retained after the
+ * call except the context's own caches (twiddle tables, generator tables).
+ *
+ * Errors.  Every function returns 0 (WBTE_OK) or a negative status; the
+ * message of the last failure is available from wbte_ctx_last_error().
+ * Results never depend on launch configuration.
+ */
+#ifndef WBTE_H
+#define WBTE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WBTE_OK 0
+#define WBTE_ERR_INVALID_ARG (-1)
+#define WBTE_ERR_SIZE (-2)
+#define WBTE_ERR_OOM (-3)
+#define WBTE_ERR_TIMEOUT (-4)
+#define WBTE_ERR_CUDA (-5)
+#define WBTE_ERR_NOT_ON_CURVE (-6)
+#define WBTE_ERR_INTERPOLATION (-7)
+
+#define WBTE_FE_FULL 0
+#define WBTE_FE_EASY 1
+#define WBTE_FE_HARD 2
+
+typedef struct wbte_ctx wbte_ctx;
+
+/* ------------------------------------------------------------ context */
+int32_t wbte_version(void);
+/* One context per GPU and caller thread.  hbm_budget_bytes = 0: no limit. */
+int32_t wbte_ctx_create(int32_t device, uint64_t hbm_budget_bytes, wbte_ctx **out);
+int32_t wbte_ctx_destroy(wbte_ctx *ctx);
+/* Use a caller-owned cudaStream_t (NULL: the context's own stream). */
+int32_t wbte_ctx_set_stream(wbte_ctx *ctx, void *cuda_stream);
+int32_t wbte_ctx_synchronize(wbte_ctx *ctx);
+const char *wbte_ctx_last_error(const wbte_ctx *ctx);
+/* Number of kernels the context has launched so far. */
+uint64_t wbte_ctx_launch_count(const wbte_ctx *ctx);
+
+/* --------------------------------------------------------------- MSM */
+/* Replaces blst_p1s_mult_pippenger with nbits = 255, one contiguous block
+ * (weighted_btx/src/blst_utils.rs:43-67 g1_multi_exp_affine_bytes).
+ * out: one G1.  n = 0 gives the identity. */
+int32_t wbte_g1_msm(wbte_ctx *ctx, void *out, const void *points, const void *scalars, uint64_t n);
+/* Replaces blst_p2s_mult_pippenger (weighted_btx/src/blst_utils.rs:88-99). */
+int32_t wbte_g2_msm(wbte_ctx *ctx, void *out, const void *points, const void *scalars, uint64_t n);
+/* k MSMs of common length n in one launch sequence:
+ *   out[j] = sum_t scalars[v_j * n + t] * points[point_base[j] + idx[t]]
+ * with idx = point_index (NULL: t) and v_j = scalar_vector[j] (NULL: 0).
+ * scalars holds num_vectors vectors of n scalars; points holds n_points.
+ * Replaces the per-block and per-index calls of
+ * weighted_btx/src/blst_utils.rs:106-152 (g2_multi_exp_affine_indexed,
+ * g2_multi_exp_affine_raw) as issued by weighted_btx/src/decryption.rs:463-521.
+ * point_base (k entries), point_index (n) and scalar_vector (k) are host. */
+int32_t wbte_g1_msm_family(wbte_ctx *ctx, void *out, const void *points, uint64_t n_points,
+                           const int64_t *point_base, const int32_t *point_index,
+                           const void *scalars, const int32_t *scalar_vector, int32_t num_vectors,
+                           uint64_t k, uint64_t n);
+int32_t wbte_g2_msm_family(wbte_ctx *ctx, void *out, const void *points, uint64_t n_points,
+                           const int64_t *point_base, const int32_t *point_index,
+                           const void *scalars, const int32_t *scalar_vector, int32_t num_vectors,
+                           uint64_t k, uint64_t n);
+
+/* ------------------------------------------------- point arithmetic */
+/* out[i] = scalars[i] * points[fixed_base ? 0 : i], affine out
+ * (blstrs G1Projective * Scalar followed by blst_p1s_to_affine,
+ * weighted_btx/src/blst_utils.rs:11-36). */
+int32_t wbte_g1_mul(wbte_ctx *ctx, void *out, const void *points, int32_t fixed_base, const void *scalars, uint64_t n);
+int32_t wbte_g2_mul(wbte_ctx *ctx, void *out, const void *points, int32_t fixed_base, const void *scalars, uint64_t n);
+/* out[i] = scalars[i] * generator (G1Projective::generator() * s,
+ * weighted_btx/src/encryption.rs:34 and setup.rs:476-484 append_g2_block). */
+int32_t wbte_g1_mul_generator(wbte_ctx *ctx, void *out, const void *scalars, uint64_t n);
+int32_t wbte_g2_mul_generator(wbte_ctx *ctx, void *out, const void *scalars, uint64_t n);
+/* out[j] = sum of in[offsets[j] .. offsets[j+1]) (offsets host, k+1 entries). */
+int32_t wbte_g1_sum(wbte_ctx *ctx, void *out, const void *in, const int64_t *offsets, uint64_t k);
+int32_t wbte_g2_sum(wbte_ctx *ctx, void *out, const void *in, const int64_t *offsets, uint64_t k);
+/* ZCash compressed encodings, 48 / 96 bytes per point (to_compressed). */
+int32_t wbte_g1_compress(wbte_ctx *ctx, void *out, const void *in, uint64_t n);
+int32_t wbte_g2_compress(wbte_ctx *ctx, void *out, const void *in, uint64_t n);
+
+/* ------------------------------------------------------- transforms */
+/* In-place radix-2 transform of n affine points over the size-n subgroup of
+ * Fr: inverse = 0 is Radix2Domain::fft, inverse = 1 is ifft_unscaled
+ * (btx/src/fft.rs:197-234, 357-411). */
+int32_t wbte_g1_ntt(wbte_ctx *ctx, void *io, uint64_t n, int32_t inverse);
+int32_t wbte_g2_ntt(wbte_ctx *ctx, void *io, uint64_t n, int32_t inverse);
+/* In-place unscaled transform of n GT elements (ifft_gt_unscaled,
+ * btx/src/fft.rs:242-274, and the forward fft for inverse = 0). */
+int32_t wbte_gt_ntt(wbte_ctx *ctx, void *io, uint64_t n, int32_t inverse);
+/* Truncated unscaled inverse transform over easy-final-exponentiated values;
+ * the first out_count outputs are valid afterwards
+ * (ifft_cyclotomic_prefix_unscaled, btx/src/fft.rs:284-350). */
+int32_t wbte_gt_cyclotomic_prefix_ifft(wbte_ctx *ctx, void *io, uint64_t n, uint64_t out_count);
+
+/* ----------------------------------------------------------- pairing */
+/* Line tables of n G2 points: 68 lines x 288 bytes each, laid out
+ * line-major (line s of point i at offset (s * n + i) * 288).
+ * Replaces blst_precompute_lines (btx/src/final_exponentiation.rs:185-195). */
+int32_t wbte_g2_prepare_lines(wbte_ctx *ctx, void *lines, const void *q, uint64_t n);
+/* out[i] = Miller loop of (p[i], lines of point i); replaces
+ * blst_miller_loop_lines (btx/src/final_exponentiation.rs:206-219). */
+int32_t wbte_miller_loop_lines(wbte_ctx *ctx, void *out, const void *lines, const void *p, uint64_t n);
+/* out[i] = Miller loop of (p[i], q[i]). */
+int32_t wbte_miller_loop(wbte_ctx *ctx, void *out, const void *p, const void *q, uint64_t n);
+/* out[j] = product over pairs [offsets[j], offsets[j+1]) of Miller loops,
+ * identities contributing 1; replaces blst_miller_loop_n as used by
+ * unprepared_multi_miller_loop (weighted_btx/src/final_exponentiation.rs:229-274).
+ * offsets host, k+1 entries. */
+int32_t wbte_multi_miller_loop(wbte_ctx *ctx, void *out, const void *p, const void *q,
+                               const int64_t *offsets, uint64_t k);
+/* mode WBTE_FE_FULL replaces blst_final_exp; WBTE_FE_EASY / WBTE_FE_HARD are
+ * easy_final_exponentiation and hard_final_exponentiation
+ * (btx/src/final_exponentiation.rs:276-336). */
+int32_t wbte_final_exp(wbte_ctx *ctx, void *out, const void *in, uint64_t n, int32_t mode);
+/* out[i] = base[fixed_base ? 0 : i] ^ scalars[i] on GT (Gt * Scalar; the
+ * decomposed action of btx/src/fft.rs:73-154). */
+int32_t wbte_gt_pow(wbte_ctx *ctx, void *out, const void *base, int32_t fixed_base, const void *scalars, uint64_t n);
+/* out[i] = a[i] * b[i] in Fp12 (blst_fp12_mul). */
+int32_t wbte_fp12_mul(wbte_ctx *ctx, void *out, const void *a, const void *b, uint64_t n);
+/* Tagged torus encoding of GT, 289 bytes per element: 0 then zeros for the
+ * identity, else 1 then (c0 + 1) / c1 (append_gt, weighted_btx/src/encoding.rs:11-19). */
+int32_t wbte_gt_compress(wbte_ctx *ctx, void *out, const void *in, uint64_t n);
+
+/* ----------------------------------------------------------- scalars */
+/* Lagrange coefficients at zero of n distinct points
+ * (lagrange_at_zero, weighted_btx/src/interpolation.rs:31-52). */
+int32_t wbte_lagrange_at_zero(wbte_ctx *ctx, void *out, const void *points, uint64_t n);
+/* valid[i] = 1 iff [s_i] G1 == R_i + [c_i] X_i (SchnorrProof::verify,
+ * weighted_btx/src/proof.rs:56-70); c_i is the Fiat-Shamir challenge. */
+int32_t wbte_schnorr_verify(wbte_ctx *ctx, uint8_t *valid, const void *X, const void *R,
+                            const void *s, const void *c, uint64_t n);
+
+/* ---------------------------------------------------- weighted_btx */
+typedef struct {
+    const void *domain_points;     /* total_weight Fr: the virtual points       */
+    const void *verification_keys; /* max_batch_size * party_count G2            */
+    const void *negative_material; /* max_batch_size * total_weight G2            */
+    const void *positive_material; /* (max_batch_size - 1) * total_weight G2      */
+    const int64_t *party_offsets;  /* host, party_count + 1 prefix offsets        */
+    uint64_t party_count;
+    uint64_t total_weight;
+    uint64_t max_batch_size;
+} wbte_wbtx_key;
+
+/* sigma[j] = sum_i q_j^(i+1) first[i] for the T secrets q (partial_decrypt,
+ * weighted_btx/src/decryption.rs:205-233). first: batch_size G1 with the
+ * identity at invalid slots. */
+int32_t wbte_wbtx_partial_decrypt(wbte_ctx *ctx, void *sigma, const void *first, uint64_t batch_size,
+                                  const void *q, uint64_t T);
+/* *ok = 1 iff the random-linear aggregate share check passes
+ * (verify_decryption_shares_batched, weighted_btx/src/decryption.rs:358-422);
+ * with one share and challenge 1 this is verify_decryption_share (:236-272).
+ * party_indices host (T entries). */
+int32_t wbte_wbtx_verify_shares(wbte_ctx *ctx, int32_t *ok, const wbte_wbtx_key *key,
+                                const void *first, const uint8_t *valid, uint64_t batch_size,
+                                const void *sigma, const int64_t *party_indices,
+                                const void *challenges, uint64_t T);
+/* Committee preparation (prepare_decryption, weighted_btx/src/decryption.rs:427-551)
+ * for the accepted parties party_indices (host, ascending):
+ *   kernel_lines  m * 68 * 288 bytes, m = next_pow2(2 batch_size)
+ *   opening_keys  batch_size * T G2, slot-major
+ *   kernel        m G2 (the scaled transformed kernel), may be NULL. */
+int32_t wbte_wbtx_prepare(wbte_ctx *ctx, const wbte_wbtx_key *key, const int64_t *party_indices, uint64_t T,
+                          uint64_t batch_size, void *kernel_lines, void *opening_keys, void *kernel);
+/* beta[i] (precompute_batch, weighted_btx/src/decryption.rs:555-603); first
+ * carries the identity at invalid slots, beta is the identity there. */
+int32_t wbte_wbtx_precompute(wbte_ctx *ctx, void *beta, const void *kernel_lines, const void *first,
+                             const uint8_t *valid, uint64_t batch_size);
+/* messages[i] = second[i] - alpha_i + beta[i] for valid slots (open_batch,
+ * weighted_btx/src/decryption.rs:607-695); invalid slots get the identity. */
+int32_t wbte_wbtx_open(wbte_ctx *ctx, void *messages, const void *opening_keys, const void *sigma, uint64_t T,
+                       const void *second, const void *beta, const uint8_t *valid, uint64_t batch_size);
+/* Public key material of keygen_with_rng (weighted_btx/src/setup.rs:98-233):
+ *   verification_keys[i * N + j] = [q_pos[i * N + j]] G2            (i < L)
+ *   negative[i * W + w]          = [z[w] q_neg[i * N + owner[w]]] G2 (i < L)
+ *   positive[i * W + w]          = [z[w] q_pos[i * N + owner[w]]] G2 (i < L - 1)
+ * owner host (W entries). */
+int32_t wbte_wbtx_keygen_material(wbte_ctx *ctx, const void *z, const int32_t *owner, const void *q_pos,
+                                  const void *q_neg, uint64_t W, uint64_t N, uint64_t L,
+                                  void *verification_keys, void *negative, void *positive);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WBTE_H */

@@ -1,0 +1,181 @@
+"""Parity of the libwbte primitives with the CPU oracle on seeded inputs.
+
+Every comparison is bit-exact on blst's memory layout (Montgomery Fp limbs),
+which is canonical for affine points and for Fp12 values.
+"""
+import random
+
+import pytest
+
+from weighted_bte_b200 import ops
+
+pytestmark = pytest.mark.gpu
+
+
+def rs(rng, n, R):
+    return [rng.randrange(R) for _ in range(n)]
+
+
+@pytest.fixture(scope="module")
+def pts(orc):
+    rng = random.Random(11)
+    g1 = orc.g1_mul_many(orc.g1_generator(), rs(rng, 64, orc.R))
+    g2 = orc.g2_mul_many(orc.g2_generator(), rs(rng, 64, orc.R))
+    return g1, g2
+
+
+def test_fixed_base_mul_matches_oracle(orc):
+    rng = random.Random(1)
+    sc = rs(rng, 37, orc.R) + [0, 1, orc.R - 1]
+    assert ops.split(ops.g1_mul_generator(sc), 96) == orc.g1_mul_many(orc.g1_generator(), sc)
+    assert ops.split(ops.g2_mul_generator(sc), 192) == orc.g2_mul_many(orc.g2_generator(), sc)
+
+
+def test_variable_base_mul_matches_oracle(orc, pts):
+    rng = random.Random(2)
+    g1, g2 = pts
+    sc = rs(rng, len(g1), orc.R)
+    assert ops.split(ops.g1_mul(b"".join(g1), sc), 96) == orc.g1_mul_many(g1, sc)
+    assert ops.split(ops.g2_mul(b"".join(g2), sc), 192) == orc.g2_mul_many(g2, sc)
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 7, 64, 513, 3000])
+def test_g1_msm_matches_oracle(orc, n):
+    rng = random.Random(100 + n)
+    points = orc.g1_mul_many(orc.g1_generator(), rs(rng, n, orc.R)) if n else []
+    sc = rs(rng, n, orc.R)
+    if n > 3:
+        points[1] = orc.G1_IDENTITY
+        points[2] = points[3]
+        sc[2] = sc[3]
+    expect = orc.g1_msm(points, sc) if n else orc.G1_IDENTITY
+    assert ops.g1_msm(b"".join(points) or b"\0" * 96, sc) == expect
+
+
+@pytest.mark.parametrize("n", [1, 5, 300])
+def test_g2_msm_matches_oracle(orc, n):
+    rng = random.Random(200 + n)
+    points = orc.g2_mul_many(orc.g2_generator(), rs(rng, n, orc.R))
+    sc = rs(rng, n, orc.R)
+    assert ops.g2_msm(b"".join(points), sc) == orc.g2_msm(points, sc)
+
+
+def test_msm_family_indexed_and_vectors(orc, pts):
+    g1, g2 = pts
+    rng = random.Random(3)
+    n, k, V = 9, 5, 2
+    idx = rng.sample(range(20), n)
+    base = [0, 7, 20, 44, 3]
+    vsel = [0, 1, 1, 0, 1]
+    scal = rs(rng, V * n, orc.R)
+    for group, bank, size, msm in ((1, g1, 96, orc.g1_msm), (2, g2, 192, orc.g2_msm)):
+        got = ops.split(ops.msm_family(group, b"".join(bank), len(bank), base, idx, scal, vsel, V, n), size)
+        for j in range(k):
+            pj = [bank[base[j] + t] for t in idx]
+            sj = scal[vsel[j] * n : (vsel[j] + 1) * n]
+            assert got[j] == msm(pj, sj), (group, j)
+
+
+def test_compressed_encodings_match_oracle(orc, pts):
+    g1, g2 = pts
+    g1 = g1[:8] + [orc.G1_IDENTITY]
+    g2 = g2[:8] + [orc.G2_IDENTITY]
+    assert ops.split(ops.g1_compress(b"".join(g1)), 48) == [orc.g1_compress(p) for p in g1]
+    assert ops.split(ops.g2_compress(b"".join(g2)), 96) == [orc.g2_compress(p) for p in g2]
+
+
+def test_pairing_matches_oracle(orc, pts):
+    g1, g2 = pts
+    P = g1[:6] + [orc.G1_IDENTITY, g1[0]]
+    Q = g2[:6] + [g2[1], orc.G2_IDENTITY]
+    got = ops.split(ops.final_exp(ops.miller_loop(b"".join(P), b"".join(Q))), 576)
+    for a, b, v in zip(P, Q, got):
+        assert v == orc.pairing(a, b)
+
+
+def test_prepared_lines_match_direct_loop(orc, pts):
+    g1, g2 = pts
+    P, Q = g1[:5] + [g1[5]], g2[:5] + [orc.G2_IDENTITY]
+    lines = ops.prepare_lines(b"".join(Q))
+    a = ops.miller_loop_lines(lines, b"".join(P))
+    b = ops.miller_loop(b"".join(P), b"".join(Q))
+    assert a == b
+    assert ops.split(ops.final_exp(a), 576) == [orc.pairing(x, y) for x, y in zip(P, Q)]
+
+
+def test_final_exponentiation_parts_match_oracle(orc, pts):
+    g1, g2 = pts
+    fs = [orc.miller_loop(g1[i], g2[i]) for i in range(4)]
+    easy = ops.split(ops.final_exp(b"".join(fs), mode=1), 576)
+    assert easy == [orc.easy_final_exp(f) for f in fs]
+    hard = ops.split(ops.final_exp(b"".join(easy), mode=2), 576)
+    assert hard == [orc.hard_final_exp(e) for e in easy]
+    full = ops.split(ops.final_exp(b"".join(fs)), 576)
+    assert full == [orc.final_exp(f) for f in fs]
+
+
+def test_multi_miller_matches_oracle(orc, pts):
+    g1, g2 = pts
+    groups = [(g1[0:3], g2[0:3]), ([], []), ([g1[4], orc.G1_IDENTITY], [g2[4], g2[5]])]
+    P = b"".join(b"".join(a) for a, _ in groups)
+    Q = b"".join(b"".join(b) for _, b in groups)
+    offs = [0, 3, 3, 5]
+    got = ops.split(ops.final_exp(ops.multi_miller_loop(P, Q, offs)), 576)
+    expect = orc.final_exp_many(orc.multi_miller_many(groups))
+    assert got == expect
+
+
+def test_gt_pow_matches_oracle(orc):
+    rng = random.Random(5)
+    e = orc.pairing(orc.g1_generator(), orc.g2_generator())
+    sc = rs(rng, 12, orc.R) + [0, 1, orc.R - 1, 0xD201000000010000]
+    got = ops.split(ops.gt_pow(e, sc, fixed_base=True), 576)
+    assert got == [orc.fp12_pow(e, s) for s in sc]
+
+
+@pytest.mark.parametrize("n", [2, 8, 32])
+def test_group_ntt_matches_oracle(orc, n):
+    rng = random.Random(300 + n)
+    g1 = orc.g1_mul_many(orc.g1_generator(), rs(rng, n, orc.R))
+    g2 = orc.g2_mul_many(orc.g2_generator(), rs(rng, n, orc.R))
+    g1[0] = orc.G1_IDENTITY
+    for inv in (False, True):
+        assert ops.split(ops.g1_ntt(b"".join(g1), inverse=inv), 96) == orc.g1_ntt(g1, inverse=inv)
+        assert ops.split(ops.g2_ntt(b"".join(g2), inverse=inv), 192) == orc.g2_ntt(g2, inverse=inv)
+
+
+@pytest.mark.parametrize("n", [2, 16])
+def test_gt_transforms_match_oracle(orc, n):
+    rng = random.Random(400 + n)
+    e = orc.pairing(orc.g1_generator(), orc.g2_generator())
+    vals = orc.gt_pow_many(e, rs(rng, n, orc.R))
+    for inv in (False, True):
+        assert ops.split(ops.gt_ntt(b"".join(vals), inverse=inv), 576) == orc.gt_ntt(vals, inverse=inv)
+    # truncated cyclotomic transform agrees after the hard part
+    g1 = orc.g1_mul_many(orc.g1_generator(), rs(rng, n, orc.R))
+    g2 = orc.g2_mul_many(orc.g2_generator(), rs(rng, n, orc.R))
+    easy = [orc.easy_final_exp(orc.miller_loop(a, b)) for a, b in zip(g1, g2)]
+    k = n // 2
+    got = ops.split(ops.final_exp(ops.cyclotomic_prefix_ifft(b"".join(easy), k), mode=2), 576)
+    expect = orc.hard_final_exp_many(orc.cyclotomic_prefix_ifft(easy, k))
+    assert got == expect
+
+
+def test_lagrange_matches_oracle(orc):
+    rng = random.Random(6)
+    xs = rs(rng, 70, orc.R)
+    assert ops.lagrange_at_zero(xs) == orc.lagrange_at_zero(xs)
+
+
+def test_schnorr_verify(orc):
+    rng = random.Random(7)
+    n = 6
+    r = rs(rng, n, orc.R)
+    k = rs(rng, n, orc.R)
+    c = rs(rng, n, orc.R)
+    s = [(ki + ci * ri) % orc.R for ki, ci, ri in zip(k, c, r)]
+    X = orc.g1_mul_many(orc.g1_generator(), r)
+    Rc = orc.g1_mul_many(orc.g1_generator(), k)
+    s[2] = (s[2] + 1) % orc.R
+    ok = ops.schnorr_verify(b"".join(X), b"".join(Rc), s, c)
+    assert list(ok) == [True, True, False, True, True, True]

@@ -1,0 +1,246 @@
+"""ctypes binding of libwbte (include/wbte.h).
+
+The library is the product's only compute path: there is no CPU fallback.
+If libwbte.so is missing, importing a compute entry point raises
+`LibraryMissing` -- build it with `python -m weighted_bte_b200.build`.
+
+Buffers: every data argument may be `bytes`/`bytearray`/`memoryview`, a
+NumPy array, a torch tensor (host or CUDA), or a raw integer address.  The
+library itself decides whether an address is device or host memory.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libwbte.so")
+
+WBTE_OK = 0
+STATUS_NAMES = {
+    -1: "WBTE_ERR_INVALID_ARG",
+    -2: "WBTE_ERR_SIZE",
+    -3: "WBTE_ERR_OOM",
+    -4: "WBTE_ERR_TIMEOUT",
+    -5: "WBTE_ERR_CUDA",
+    -6: "WBTE_ERR_NOT_ON_CURVE",
+    -7: "WBTE_ERR_INTERPOLATION",
+}
+FE_FULL, FE_EASY, FE_HARD = 0, 1, 2
+G1_BYTES, G2_BYTES, GT_BYTES, FR_BYTES, LINE_BYTES, MILLER_LINES = 96, 192, 576, 32, 288, 68
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+class WbteError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class WbtxKey(ctypes.Structure):
+    _fields_ = [
+        ("domain_points", ctypes.c_void_p),
+        ("verification_keys", ctypes.c_void_p),
+        ("negative_material", ctypes.c_void_p),
+        ("positive_material", ctypes.c_void_p),
+        ("party_offsets", ctypes.c_void_p),
+        ("party_count", ctypes.c_uint64),
+        ("total_weight", ctypes.c_uint64),
+        ("max_batch_size", ctypes.c_uint64),
+    ]
+
+
+_VP, _U64, _I32, _I64 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int64
+# name -> argument types after the context pointer
+_SIGNATURES = {
+    "wbte_g1_msm": [_VP, _VP, _VP, _U64],
+    "wbte_g2_msm": [_VP, _VP, _VP, _U64],
+    "wbte_g1_msm_family": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _I32, _U64, _U64],
+    "wbte_g2_msm_family": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _I32, _U64, _U64],
+    "wbte_g1_mul": [_VP, _VP, _I32, _VP, _U64],
+    "wbte_g2_mul": [_VP, _VP, _I32, _VP, _U64],
+    "wbte_g1_mul_generator": [_VP, _VP, _U64],
+    "wbte_g2_mul_generator": [_VP, _VP, _U64],
+    "wbte_g1_sum": [_VP, _VP, _VP, _U64],
+    "wbte_g2_sum": [_VP, _VP, _VP, _U64],
+    "wbte_g1_compress": [_VP, _VP, _U64],
+    "wbte_g2_compress": [_VP, _VP, _U64],
+    "wbte_g1_ntt": [_VP, _U64, _I32],
+    "wbte_g2_ntt": [_VP, _U64, _I32],
+    "wbte_gt_ntt": [_VP, _U64, _I32],
+    "wbte_gt_cyclotomic_prefix_ifft": [_VP, _U64, _U64],
+    "wbte_g2_prepare_lines": [_VP, _VP, _U64],
+    "wbte_miller_loop_lines": [_VP, _VP, _VP, _U64],
+    "wbte_miller_loop": [_VP, _VP, _VP, _U64],
+    "wbte_multi_miller_loop": [_VP, _VP, _VP, _VP, _U64],
+    "wbte_final_exp": [_VP, _VP, _U64, _I32],
+    "wbte_gt_pow": [_VP, _VP, _I32, _VP, _U64],
+    "wbte_fp12_mul": [_VP, _VP, _VP, _U64],
+    "wbte_gt_compress": [_VP, _VP, _U64],
+    "wbte_lagrange_at_zero": [_VP, _VP, _U64],
+    "wbte_schnorr_verify": [_VP, _VP, _VP, _VP, _VP, _U64],
+    "wbte_wbtx_partial_decrypt": [_VP, _VP, _U64, _VP, _U64],
+    "wbte_wbtx_verify_shares": [_VP, _VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64],
+    "wbte_wbtx_prepare": [_VP, _VP, _U64, _U64, _VP, _VP, _VP],
+    "wbte_wbtx_precompute": [_VP, _VP, _VP, _VP, _U64],
+    "wbte_wbtx_open": [_VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64],
+    "wbte_wbtx_keygen_material": [_VP, _VP, _VP, _VP, _U64, _U64, _U64, _VP, _VP, _VP],
+}
+EXPORTED = sorted(
+    list(_SIGNATURES)
+    + ["wbte_version", "wbte_ctx_create", "wbte_ctx_destroy", "wbte_ctx_set_stream", "wbte_ctx_synchronize",
+       "wbte_ctx_last_error", "wbte_ctx_launch_count"]
+)
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Load libwbte.so (raises LibraryMissing if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise LibraryMissing(
+                f"{LIB_PATH} is missing: the CUDA library must be built "
+                "(python -m weighted_bte_b200.build); there is no CPU fallback"
+            )
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.wbte_version.restype = _I32
+        lib.wbte_ctx_create.argtypes = [_I32, _U64, ctypes.POINTER(_VP)]
+        lib.wbte_ctx_create.restype = _I32
+        lib.wbte_ctx_destroy.argtypes = [_VP]
+        lib.wbte_ctx_destroy.restype = _I32
+        lib.wbte_ctx_set_stream.argtypes = [_VP, _VP]
+        lib.wbte_ctx_set_stream.restype = _I32
+        lib.wbte_ctx_synchronize.argtypes = [_VP]
+        lib.wbte_ctx_synchronize.restype = _I32
+        lib.wbte_ctx_last_error.argtypes = [_VP]
+        lib.wbte_ctx_last_error.restype = ctypes.c_char_p
+        lib.wbte_ctx_launch_count.argtypes = [_VP]
+        lib.wbte_ctx_launch_count.restype = _U64
+        for name, args in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = [_VP] + args
+            fn.restype = _I32
+        _lib = lib
+        return lib
+
+
+class _Keep:
+    """Holds ctypes buffers alive for the duration of one call."""
+
+    def __init__(self):
+        self.items = []
+
+    def ptr(self, x):
+        if x is None:
+            return None
+        if isinstance(x, int):
+            return x
+        mod = type(x).__module__
+        if mod.startswith("torch"):
+            return x.data_ptr()
+        if isinstance(x, np.ndarray):
+            if not x.flags["C_CONTIGUOUS"]:
+                raise ValueError("arrays must be C-contiguous")
+            self.items.append(x)
+            return x.ctypes.data
+        if isinstance(x, bytes):
+            buf = ctypes.create_string_buffer(x, len(x))
+            self.items.append(buf)
+            return ctypes.addressof(buf)
+        if isinstance(x, (bytearray, memoryview)):
+            mv = memoryview(x)
+            if mv.readonly:
+                buf = ctypes.create_string_buffer(mv.tobytes(), mv.nbytes)
+                self.items.append(buf)
+                return ctypes.addressof(buf)
+            arr = (ctypes.c_char * mv.nbytes).from_buffer(mv)
+            self.items.append(arr)
+            return ctypes.addressof(arr)
+        if isinstance(x, ctypes.Array):
+            return ctypes.addressof(x)
+        raise TypeError(f"unsupported buffer type {type(x)}")
+
+
+def i64_array(values) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(values, dtype=np.int64))
+
+
+def i32_array(values) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(values, dtype=np.int32))
+
+
+class Context:
+    """A libwbte context bound to one GPU."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self.lib = load()
+        h = _VP()
+        st = self.lib.wbte_ctx_create(int(device), int(hbm_budget_bytes), ctypes.byref(h))
+        if st != WBTE_OK:
+            raise WbteError(st, f"could not create a context on device {device}")
+        self.handle = h.value
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            self.lib.wbte_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int | None):
+        self.lib.wbte_ctx_set_stream(self.handle, stream_handle or None)
+
+    def synchronize(self):
+        self._check(self.lib.wbte_ctx_synchronize(self.handle))
+
+    def launch_count(self) -> int:
+        return int(self.lib.wbte_ctx_launch_count(self.handle))
+
+    def _check(self, st: int):
+        if st != WBTE_OK:
+            msg = self.lib.wbte_ctx_last_error(self.handle)
+            raise WbteError(st, msg.decode() if msg else "")
+
+    def call(self, name: str, *args):
+        keep = _Keep()
+        conv = []
+        for a in args:
+            if isinstance(a, ctypes.Structure):
+                conv.append(ctypes.addressof(a))
+                keep.items.append(a)
+            elif isinstance(a, (bool, np.integer)):
+                conv.append(int(a))
+            elif isinstance(a, int) and not isinstance(a, bool):
+                conv.append(a)
+            else:
+                conv.append(keep.ptr(a))
+        st = getattr(self.lib, name)(self.handle, *conv)
+        self._check(st)
+        return keep
+
+
+_default = {}
+
+
+def default_context(device: int = 0) -> Context:
+    ctx = _default.get(device)
+    if ctx is None:
+        ctx = Context(device)
+        _default[device] = ctx
+    return ctx

@@ -1,0 +1,97 @@
+"""Builds libwbte.so (the sm_100a kernels and the C ABI of include/wbte.h).
+
+    python -m weighted_bte_b200.build        # incremental
+    python -m weighted_bte_b200.build --force
+
+Each .cu under csrc/ is compiled in parallel with
+`nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo` and linked
+against the static CUDA runtime, so the library does not depend on which
+libcudart another component of the process loads.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import hashlib
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libwbte.so")
+SOURCES = ["k_arith.cu", "k_msm.cu", "k_pairing.cu", "runtime.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INCLUDE]
+
+
+def nvcc() -> str:
+    path = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(path):
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libwbte")
+    return path
+
+
+def _headers_digest() -> str:
+    h = hashlib.sha256()
+    for name in sorted(os.listdir(CSRC)):
+        if name.endswith((".cuh", ".h")):
+            with open(os.path.join(CSRC, name), "rb") as f:
+                h.update(name.encode() + f.read())
+    with open(os.path.join(INCLUDE, "wbte.h"), "rb") as f:
+        h.update(f.read())
+    h.update(" ".join(ARCH + FLAGS).encode())
+    return h.hexdigest()
+
+
+def _compile(src: str, digest: str, force: bool) -> str:
+    path = os.path.join(CSRC, src)
+    with open(path, "rb") as f:
+        key = hashlib.sha256(f.read() + digest.encode()).hexdigest()[:16]
+    obj = os.path.join(BUILD, f"{src[:-3]}.{key}.o")
+    if os.path.exists(obj) and not force:
+        return obj
+    cmd = [nvcc()] + ARCH + FLAGS + ["-c", path, "-o", obj + ".tmp"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{res.stderr[-6000:]}")
+    os.replace(obj + ".tmp", obj)
+    return obj
+
+
+def build(force: bool = False, verbose: bool = True) -> str:
+    if not os.path.exists(os.path.join(CSRC, "field_asm.cuh")) or force:
+        subprocess.run([sys.executable, os.path.join(CSRC, "gen_field.py")], check=True)
+    os.makedirs(BUILD, exist_ok=True)
+    digest = _headers_digest()
+    with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(lambda s: _compile(s, digest, force), SOURCES))
+    stamp = hashlib.sha256("".join(objs).encode()).hexdigest()
+    stamp_file = os.path.join(BUILD, "link.stamp")
+    if os.path.exists(LIB) and os.path.exists(stamp_file) and not force:
+        with open(stamp_file) as f:
+            if f.read() == stamp:
+                return LIB
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB + ".tmp"] + objs + ["-cudart", "static"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"link failed:\n{res.stderr[-6000:]}")
+    os.replace(LIB + ".tmp", LIB)
+    with open(stamp_file, "w") as f:
+        f.write(stamp)
+    # drop objects of older source versions
+    keep = set(objs)
+    for name in os.listdir(BUILD):
+        p = os.path.join(BUILD, name)
+        if name.endswith(".o") and p not in keep:
+            os.remove(p)
+    if verbose:
+        print(f"built {LIB}")
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

@@ -1,0 +1,418 @@
+// Scalar-field kernels, batched point multiplication, radix-2 group
+// transforms, compressed encodings and Schnorr checks.
+#include "launch.h"
+#include "pairing.cuh"
+
+namespace wbte {
+
+namespace {
+constexpr int TPB = 128;
+inline unsigned blocks_for(int64_t n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+WBTE_INL Fr load_fr_mont(const uint8_t* p) {
+    Fr a;
+    load_scalar(a.v, p);
+    return fr_to_mont(a);
+}
+WBTE_INL void store_fr_canonical(uint8_t* p, const Fr& m) {
+    Fr a = fr_from_mont(m);
+    uint4* d = reinterpret_cast<uint4*>(p);
+    d[0] = make_uint4(a.v[0], a.v[1], a.v[2], a.v[3]);
+    d[1] = make_uint4(a.v[4], a.v[5], a.v[6], a.v[7]);
+}
+
+template <class F> struct GroupOf;
+template <> struct GroupOf<Fp> { static constexpr size_t AFF = G1_AFF; };
+template <> struct GroupOf<Fp2> { static constexpr size_t AFF = G2_AFF; };
+
+// ------------------------------------------------------------- scalars
+__global__ void k_fr_powers(uint8_t* out, const uint8_t* base, int64_t n, int64_t first) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fr b = load_fr_mont(base);
+    // base^(first + i) by square-and-multiply
+    uint64_t e = (uint64_t)(first + i);
+    Fr r = fr_pow_u64(b, e);
+    store_fr_canonical(out + FR_SZ * i, r);
+}
+
+__global__ void k_fr_mul_gather(uint8_t* out, const uint8_t* a, const uint8_t* b, const int32_t* bidx, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fr x = load_fr_mont(a + FR_SZ * i);
+    Fr y = load_fr_mont(b + FR_SZ * (bidx ? (int64_t)bidx[i] : i));
+    store_fr_canonical(out + FR_SZ * i, fr_mul(x, y));
+}
+
+__global__ void k_fr_scale(uint8_t* out, const uint8_t* a, const uint8_t* c, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    store_fr_canonical(out + FR_SZ * i, fr_mul(load_fr_mont(a + FR_SZ * i), load_fr_mont(c)));
+}
+
+__global__ void k_fr_scale_size_inv(uint8_t* out, const uint8_t* a, int log_m, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fr c;
+    _Pragma("unroll") for (int t = 0; t < 8; t++) c.v[t] = C_DOMAIN_SIZE_INV[log_m][t];
+    store_fr_canonical(out + FR_SZ * i, fr_mul(load_fr_mont(a + FR_SZ * i), c));
+}
+
+__global__ void k_material_scalars(uint8_t* out, const uint8_t* z, const int32_t* owner, const uint8_t* qp,
+                                   int64_t W, int64_t N, int64_t rows) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= rows * W) return;
+    int64_t r = i / W, w = i % W;
+    Fr x = load_fr_mont(z + FR_SZ * w);
+    Fr y = load_fr_mont(qp + FR_SZ * (r * N + owner[w]));
+    store_fr_canonical(out + FR_SZ * i, fr_mul(x, y));
+}
+
+__global__ void k_gather(uint8_t* out, const uint8_t* in, const int32_t* idx, int64_t n, int64_t record) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint8_t* src = in + record * (int64_t)idx[i];
+    uint8_t* dst = out + record * i;
+    if ((record & 15) == 0) {
+        for (int64_t b = 0; b < record; b += 16)
+            *reinterpret_cast<uint4*>(dst + b) = *reinterpret_cast<const uint4*>(src + b);
+    } else {
+        for (int64_t b = 0; b < record; b++) dst[b] = src[b];
+    }
+}
+
+// L_i(0) = prod_{k != i} (-x_k) / (x_i - x_k)
+__global__ void k_lagrange(uint8_t* out, const uint8_t* x, int64_t n, int32_t* status) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fr xi = load_fr_mont(x + FR_SZ * i);
+    Fr num = fr_one(), den = fr_one();
+    for (int64_t k = 0; k < n; k++) {
+        if (k == i) continue;
+        Fr xk = load_fr_mont(x + FR_SZ * k);
+        num = fr_mul(num, fr_neg(xk));
+        den = fr_mul(den, fr_sub(xi, xk));
+    }
+    if (fr_is_zero(den)) {
+        atomicExch(status, 1);
+        return;
+    }
+    store_fr_canonical(out + FR_SZ * i, fr_mul(num, fr_inv(den)));
+}
+
+__global__ void k_domain_twiddles(uint8_t* tw, int log_n, int64_t count, bool inverse) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    Fr g;
+    _Pragma("unroll") for (int i = 0; i < 8; i++) g.v[i] = inverse ? C_DOMAIN_GEN_INV[log_n][i] : C_DOMAIN_GEN[log_n][i];
+    store_fr_canonical(tw + FR_SZ * j, fr_pow_u64(g, (uint64_t)j));
+}
+
+// -------------------------------------------------------------- points
+template <class F>
+__global__ void k_mul_batch(uint8_t* out, const uint8_t* pts, int64_t stride, const uint8_t* scalars, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    using A = Affine<F>;
+    A p = load_affine(reinterpret_cast<const A*>(pts + stride * i * GroupOf<F>::AFF));
+    uint32_t k[8];
+    load_scalar(k, scalars + FR_SZ * i);
+    Xyzz<F> r = xyzz_mul(from_affine(p), k);
+    store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * i), to_affine(r));
+}
+
+template <class F> WBTE_INL Affine<F> generator_of();
+template <> WBTE_INL Affine<Fp> generator_of<Fp>() { return g1_generator(); }
+template <> WBTE_INL Affine<Fp2> generator_of<Fp2>() { return g2_generator(); }
+
+// Fixed-base multiplication by the generator with a table of
+// T[w][d] = d * 2^(8w) * G (w < 32, d < 256), one mixed addition per window.
+template <class F>
+__global__ void k_build_gen_table(uint8_t* table) {
+    int w = blockIdx.x;  // 0..31
+    int d = threadIdx.x; // 0..255
+    using A = Affine<F>;
+    Xyzz<F> base = from_affine(generator_of<F>());
+    for (int i = 0; i < 8 * w; i++) base = xyzz_dbl(base);
+    Xyzz<F> r = xyzz_mul_u64(base, (uint64_t)d);
+    store_affine(reinterpret_cast<A*>(table + GroupOf<F>::AFF * (256 * w + d)), to_affine(r));
+}
+
+template <class F>
+__global__ void k_mul_generator(uint8_t* out, const uint8_t* table, const uint8_t* scalars, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    using A = Affine<F>;
+    const A* T = reinterpret_cast<const A*>(table);
+    const uint8_t* s = scalars + FR_SZ * i;
+    Xyzz<F> acc;
+    set_inf(acc);
+    for (int w = 0; w < 32; w++) {
+        uint32_t d = s[w];
+        if (d) acc = xyzz_madd(acc, load_affine(T + 256 * w + d));
+    }
+    store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * i), to_affine(acc));
+}
+
+template <class F>
+__global__ void k_mul_pow2(uint8_t* out, const uint8_t* in, int64_t n, int k) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    using A = Affine<F>;
+    Xyzz<F> r = from_affine(load_affine(reinterpret_cast<const A*>(in + GroupOf<F>::AFF * i)));
+    for (int t = 0; t < k; t++) r = xyzz_dbl(r);
+    store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * i), to_affine(r));
+}
+
+template <class F>
+__global__ void k_segment_sum(uint8_t* out, const uint8_t* in, const int64_t* offsets, int64_t k) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    using A = Affine<F>;
+    Xyzz<F> acc;
+    set_inf(acc);
+    for (int64_t t = offsets[j]; t < offsets[j + 1]; t++)
+        acc = xyzz_madd(acc, load_affine(reinterpret_cast<const A*>(in + GroupOf<F>::AFF * t)));
+    store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * j), to_affine(acc));
+}
+
+template <class F>
+__global__ void k_negate(uint8_t* out, const uint8_t* in, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    using A = Affine<F>;
+    A p = load_affine(reinterpret_cast<const A*>(in + GroupOf<F>::AFF * i));
+    store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * i), neg(p));
+}
+
+// ----------------------------------------------------- group transforms
+__device__ __forceinline__ int64_t bitrev64(int64_t i, int bits) {
+    return bits ? (int64_t)(__brevll((unsigned long long)i) >> (64 - bits)) : 0;
+}
+
+template <class F>
+__global__ void k_ntt_load(uint8_t* work, const uint8_t* in, int64_t n, int bits) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    using A = Affine<F>;
+    Xyzz<F> p = from_affine(load_affine(reinterpret_cast<const A*>(in + GroupOf<F>::AFF * i)));
+    store_vec(reinterpret_cast<Xyzz<F>*>(work) + bitrev64(i, bits), p);
+}
+
+// one radix-2 butterfly per thread; twiddle index j * (n / size)
+template <class F>
+__global__ void k_ntt_stage(uint8_t* work, const uint8_t* tw, int64_t n, int64_t half) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n / 2) return;
+    int64_t chunk = t / half, j = t % half;
+    Xyzz<F>* w = reinterpret_cast<Xyzz<F>*>(work);
+    int64_t a = chunk * 2 * half + j, b = a + half;
+    Xyzz<F> u = load_vec(w + a), v = load_vec(w + b);
+    if (j != 0) {
+        uint32_t k[8];
+        load_scalar(k, tw + FR_SZ * (j * (n / (2 * half))));
+        v = xyzz_mul(v, k);
+    }
+    store_vec(w + a, xyzz_add(u, v));
+    store_vec(w + b, xyzz_add(u, neg(v)));
+}
+
+template <class F>
+__global__ void k_xyzz_to_affine(uint8_t* out, const uint8_t* work, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    using A = Affine<F>;
+    Xyzz<F> p = load_vec(reinterpret_cast<const Xyzz<F>*>(work) + i);
+    store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * i), to_affine(p));
+}
+
+// ------------------------------------------------------------ encodings
+WBTE_INL void fp_store_be48(uint8_t* out, const Fp& m) {
+    Fp c = fp_from_mont(m);
+    for (int i = 0; i < 48; i++) out[47 - i] = (uint8_t)(c.v[i >> 2] >> (8 * (i & 3)));
+}
+WBTE_INL bool fp_largest(const Fp& m) {
+    Fp c = fp_from_mont(m);
+    for (int i = 11; i >= 0; i--) {
+        if (c.v[i] != C_P_HALF[i]) return c.v[i] > C_P_HALF[i];
+    }
+    return false;
+}
+__global__ void k_g1_compress(uint8_t* out, const uint8_t* in, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    G1A p = load_affine(reinterpret_cast<const G1A*>(in + G1_AFF * i));
+    uint8_t* o = out + 48 * i;
+    if (is_inf(p)) {
+        for (int b = 0; b < 48; b++) o[b] = 0;
+        o[0] = 0xc0;
+        return;
+    }
+    fp_store_be48(o, p.x);
+    o[0] |= 0x80 | (fp_largest(p.y) ? 0x20 : 0);
+}
+__global__ void k_g2_compress(uint8_t* out, const uint8_t* in, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    G2A p = load_affine(reinterpret_cast<const G2A*>(in + G2_AFF * i));
+    uint8_t* o = out + 96 * i;
+    if (is_inf(p)) {
+        for (int b = 0; b < 96; b++) o[b] = 0;
+        o[0] = 0xc0;
+        return;
+    }
+    fp_store_be48(o, p.x.c1);
+    fp_store_be48(o + 48, p.x.c0);
+    bool largest = fp_is_zero(p.y.c1) ? fp_largest(p.y.c0) : fp_largest(p.y.c1);
+    o[0] |= 0x80 | (largest ? 0x20 : 0);
+}
+
+__global__ void k_schnorr_verify(uint8_t* valid, const uint8_t* X, const uint8_t* R, const uint8_t* sresp,
+                                 const uint8_t* c, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t ks[8], kc[8];
+    load_scalar(ks, sresp + FR_SZ * i);
+    load_scalar(kc, c + FR_SZ * i);
+    G1X lhs = xyzz_mul(from_affine(g1_generator()), ks);
+    G1X cx = xyzz_mul(from_affine(load_affine(reinterpret_cast<const G1A*>(X + G1_AFF * i))), kc);
+    G1A r = load_affine(reinterpret_cast<const G1A*>(R + G1_AFF * i));
+    G1X rhs = xyzz_madd(cx, r);
+    G1X diff = xyzz_add(lhs, neg(rhs));
+    valid[i] = is_inf(diff) ? 1 : 0;
+}
+
+}  // namespace
+
+// ============================================================ launchers
+void launch_fr_powers(uint8_t* out, const uint8_t* base, int64_t n, int64_t first, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_fr_powers<<<blocks_for(n), TPB, 0, s>>>(out, base, n, first);
+}
+void launch_fr_mul_gather(uint8_t* out, const uint8_t* a, const uint8_t* b, const int32_t* bidx, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_fr_mul_gather<<<blocks_for(n), TPB, 0, s>>>(out, a, b, bidx, n);
+}
+void launch_fr_scale(uint8_t* out, const uint8_t* a, const uint8_t* c, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_fr_scale<<<blocks_for(n), TPB, 0, s>>>(out, a, c, n);
+}
+void launch_fr_scale_size_inv(uint8_t* out, const uint8_t* a, int log_m, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_fr_scale_size_inv<<<blocks_for(n), TPB, 0, s>>>(out, a, log_m, n);
+}
+void launch_material_scalars(uint8_t* out, const uint8_t* z, const int32_t* owner, const uint8_t* qp, int64_t W,
+                             int64_t N, int64_t rows, cudaStream_t s) {
+    if (rows * W <= 0) return;
+    note_launch();
+    k_material_scalars<<<blocks_for(rows * W), TPB, 0, s>>>(out, z, owner, qp, W, N, rows);
+}
+void launch_gather(uint8_t* out, const uint8_t* in, const int32_t* idx, int64_t n, int64_t record, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_gather<<<blocks_for(n), TPB, 0, s>>>(out, in, idx, n, record);
+}
+void launch_lagrange_at_zero(uint8_t* out, const uint8_t* x, int64_t n, int32_t* status, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_lagrange<<<blocks_for(n, 64), 64, 0, s>>>(out, x, n, status);
+}
+void launch_domain_twiddles(uint8_t* tw, int64_t n, int64_t count, bool inverse, cudaStream_t s) {
+    if (count <= 0) return;
+    int lg = 0;
+    while ((int64_t(1) << lg) < n) lg++;
+    note_launch();
+    k_domain_twiddles<<<blocks_for(count), TPB, 0, s>>>(tw, lg, count, inverse);
+}
+
+void launch_mul_batch(Group g, uint8_t* out, const uint8_t* pts, int64_t stride, const uint8_t* scalars, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    if (g == GROUP_G1) k_mul_batch<Fp><<<blocks_for(n), TPB, 0, s>>>(out, pts, stride, scalars, n);
+    else k_mul_batch<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, pts, stride, scalars, n);
+}
+
+// generator tables are built once per device on first use
+static uint8_t* g_gen_table[2][64] = {};
+void launch_mul_generator(Group g, uint8_t* out, const uint8_t* scalars, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int gi = g == GROUP_G1 ? 0 : 1;
+    size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    if (!g_gen_table[gi][dev]) {
+        uint8_t* t = nullptr;
+        if (cudaMalloc(&t, aff * 256 * 32) != cudaSuccess) return;
+        note_launch();
+        if (g == GROUP_G1) k_build_gen_table<Fp><<<32, 256, 0, s>>>(t);
+        else k_build_gen_table<Fp2><<<32, 256, 0, s>>>(t);
+        g_gen_table[gi][dev] = t;
+    }
+    note_launch();
+    if (g == GROUP_G1) k_mul_generator<Fp><<<blocks_for(n), TPB, 0, s>>>(out, g_gen_table[gi][dev], scalars, n);
+    else k_mul_generator<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, g_gen_table[gi][dev], scalars, n);
+}
+
+void launch_mul_pow2(Group g, uint8_t* out, const uint8_t* in, int64_t n, int k, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    if (g == GROUP_G1) k_mul_pow2<Fp><<<blocks_for(n), TPB, 0, s>>>(out, in, n, k);
+    else k_mul_pow2<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, in, n, k);
+}
+void launch_segment_sum(Group g, uint8_t* out, const uint8_t* in, const int64_t* offsets, int64_t k, cudaStream_t s) {
+    if (k <= 0) return;
+    note_launch();
+    if (g == GROUP_G1) k_segment_sum<Fp><<<blocks_for(k), TPB, 0, s>>>(out, in, offsets, k);
+    else k_segment_sum<Fp2><<<blocks_for(k), TPB, 0, s>>>(out, in, offsets, k);
+}
+void launch_negate(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    if (g == GROUP_G1) k_negate<Fp><<<blocks_for(n), TPB, 0, s>>>(out, in, n);
+    else k_negate<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, in, n);
+}
+
+void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    int bits = 0;
+    while ((int64_t(1) << bits) < n) bits++;
+    if (g == GROUP_G1) {
+        note_launch();
+        k_ntt_load<Fp><<<blocks_for(n), TPB, 0, s>>>(work, io, n, bits);
+        for (int64_t half = 1; half < n; half *= 2) {
+            note_launch();
+            k_ntt_stage<Fp><<<blocks_for(n / 2, 64), 64, 0, s>>>(work, tw, n, half);
+        }
+        note_launch();
+        k_xyzz_to_affine<Fp><<<blocks_for(n), TPB, 0, s>>>(io, work, n);
+    } else {
+        note_launch();
+        k_ntt_load<Fp2><<<blocks_for(n), TPB, 0, s>>>(work, io, n, bits);
+        for (int64_t half = 1; half < n; half *= 2) {
+            note_launch();
+            k_ntt_stage<Fp2><<<blocks_for(n / 2, 64), 64, 0, s>>>(work, tw, n, half);
+        }
+        note_launch();
+        k_xyzz_to_affine<Fp2><<<blocks_for(n), TPB, 0, s>>>(io, work, n);
+    }
+}
+
+void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    if (g == GROUP_G1) k_g1_compress<<<blocks_for(n), TPB, 0, s>>>(out, in, n);
+    else k_g2_compress<<<blocks_for(n), TPB, 0, s>>>(out, in, n);
+}
+
+void launch_schnorr_verify(uint8_t* valid, const uint8_t* X, const uint8_t* R, const uint8_t* sresp, const uint8_t* c,
+                           int64_t n, cudaStream_t st) {
+    if (n <= 0) return;
+    note_launch();
+    k_schnorr_verify<<<blocks_for(n), TPB, 0, st>>>(valid, X, R, sresp, c, n);
+}
+
+}  // namespace wbte

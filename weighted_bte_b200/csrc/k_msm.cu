@@ -1,0 +1,301 @@
+// Pippenger multi-scalar multiplication for families of equal-length MSMs.
+//
+//   out[j] = sum_t scalars[v_j][t] * points[pbase[j] + idx[t]]
+//
+// This covers blst's contiguous `p{1,2}s_mult_pippenger` blocks (one MSM,
+// idx = identity), the reference's sparse indexed G2 MSMs
+// (weighted_btx/src/blst_utils.rs:106-125: idx = accepted virtual indices,
+// one base block per kernel offset) and the per-slot party blocks of
+// weighted_btx/src/decryption.rs:463-481 (one family per party).  Scalars are
+// shared by every MSM using the same vector, so the signed-digit recoding and
+// the per-window bucket sort are done once per (vector, window).
+//
+// Pipeline:
+//  1. digits:  signed c-bit windows, digit in (-2^(c-1), 2^(c-1)]
+//  2. sort:    one CTA per (vector, window) counting-sorts term indices by
+//              |digit| in descending order (zero digits dropped)
+//  3. segments: one thread per (MSM, window, segment of S sorted terms)
+//              evaluates sum_e |d_e| * (+-P_e) over its segment with a running
+//              sum (Abel summation) -- no bucket array is materialised
+//  4. reduce:  tree sums over the segments of each (MSM, window)
+//  5. combine: Horner over windows, then conversion to affine.
+// Group addition is exact and commutative, so the result does not depend on
+// the order that atomics give terms inside a bucket.
+#include "launch.h"
+#include "pairing.cuh"
+
+namespace wbte {
+
+namespace {
+constexpr int TPB = 128;
+inline unsigned blocks_for(int64_t n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+template <class F> struct Aff;
+template <> struct Aff<Fp> { static constexpr size_t SZ = G1_AFF; };
+template <> struct Aff<Fp2> { static constexpr size_t SZ = G2_AFF; };
+
+// entry packing: term index (32 bits) | bucket (16 bits) << 32 | sign << 63
+WBTE_INL uint64_t pack_entry(uint32_t t, uint32_t b, bool negative) {
+    return (uint64_t)t | ((uint64_t)b << 32) | ((uint64_t)(negative ? 1 : 0) << 63);
+}
+
+__global__ void k_digits(int16_t* digits, const uint8_t* scalars, int64_t total, int64_t n, int c, int windows) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // i = v * n + t
+    if (i >= total) return;
+    uint32_t k[8];
+    load_scalar(k, scalars + FR_SZ * i);
+    int64_t v = i / n, t = i % n;
+    int carry = 0;
+    const int full = 1 << c, half = 1 << (c - 1);
+    for (int w = 0; w < windows; w++) {
+        int bit = w * c;
+        uint32_t val = 0;
+        if (bit < 256) {
+            int word = bit >> 5, off = bit & 31;
+            uint64_t two = (uint64_t)k[word] | ((word + 1 < 8) ? ((uint64_t)k[word + 1] << 32) : 0ull);
+            val = (uint32_t)(two >> off) & (uint32_t)(full - 1);
+        }
+        int d = (int)val + carry;
+        if (d > half) {
+            d -= full;
+            carry = 1;
+        } else {
+            carry = 0;
+        }
+        digits[(v * windows + w) * n + t] = (int16_t)d;
+    }
+}
+
+// One CTA per (vector, window).  counts lives in dynamic shared memory.
+__global__ void k_sort(uint64_t* entries, int32_t* nnz, const int16_t* digits, int64_t n, int buckets) {
+    extern __shared__ int32_t sh[];
+    int32_t* cnt = sh;                // buckets + 1
+    int32_t* cur = sh + buckets + 1;  // buckets + 1
+    int64_t vw = blockIdx.x;
+    const int16_t* d = digits + vw * n;
+    for (int b = threadIdx.x; b <= buckets; b += blockDim.x) cnt[b] = 0;
+    __syncthreads();
+    for (int64_t t = threadIdx.x; t < n; t += blockDim.x) {
+        int x = d[t];
+        atomicAdd(&cnt[x < 0 ? -x : x], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // descending bucket order; bucket 0 is dropped
+        int32_t run = 0;
+        for (int b = buckets; b >= 1; b--) {
+            cur[b] = run;
+            run += cnt[b];
+        }
+        nnz[vw] = run;
+    }
+    __syncthreads();
+    uint64_t* out = entries + vw * n;
+    for (int64_t t = threadIdx.x; t < n; t += blockDim.x) {
+        int x = d[t];
+        int b = x < 0 ? -x : x;
+        if (b == 0) continue;
+        int32_t pos = atomicAdd(&cur[b], 1);
+        out[pos] = pack_entry((uint32_t)t, (uint32_t)b, x < 0);
+    }
+}
+
+// acc += g * run for a small positive g
+template <class F> WBTE_INL Xyzz<F> add_small_multiple(const Xyzz<F>& acc, const Xyzz<F>& run, uint32_t g) {
+    if (g == 1) return xyzz_add(acc, run);
+    Xyzz<F> m;
+    set_inf(m);
+    int top = 31 - __clz(g);
+    for (int b = top; b >= 0; b--) {
+        m = xyzz_dbl(m);
+        if ((g >> b) & 1) m = xyzz_add(m, run);
+    }
+    return xyzz_add(acc, m);
+}
+
+template <class F>
+__global__ void k_segments(uint8_t* seg_out, const uint8_t* points, const int64_t* pbase, const int32_t* idx,
+                           const uint64_t* entries, const int32_t* nnz, const int32_t* vsel,
+                           int64_t k, int64_t n, int windows, int64_t S, int64_t nseg) {
+    int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t total = k * windows * nseg;
+    if (gid >= total) return;
+    int64_t seg = gid % nseg;
+    int64_t w = (gid / nseg) % windows;
+    int64_t j = gid / (nseg * windows);
+    int64_t v = vsel ? vsel[j] : 0;
+    int64_t vw = v * windows + w;
+    int64_t lo = seg * S, hi = lo + S;
+    int64_t cnt = nnz[vw];
+    if (hi > cnt) hi = cnt;
+    using A = Affine<F>;
+    Xyzz<F> run, acc;
+    set_inf(run);
+    set_inf(acc);
+    if (lo < hi) {
+        const uint64_t* e = entries + vw * n;
+        const A* P = reinterpret_cast<const A*>(points) + pbase[j];
+        uint32_t cur_b = (uint32_t)(e[lo] >> 32) & 0x7fffu;
+        for (int64_t x = lo; x < hi; x++) {
+            uint64_t en = e[x];
+            uint32_t b = (uint32_t)(en >> 32) & 0x7fffu;
+            uint32_t t = (uint32_t)en;
+            if (b != cur_b) {
+                acc = add_small_multiple(acc, run, cur_b - b);
+                cur_b = b;
+            }
+            A p = load_affine(P + (idx ? (int64_t)idx[t] : (int64_t)t));
+            if (en >> 63) p = neg(p);
+            run = xyzz_madd(run, p);
+        }
+        acc = add_small_multiple(acc, run, cur_b);
+    }
+    store_vec(reinterpret_cast<Xyzz<F>*>(seg_out) + gid, acc);
+}
+
+// out[i] = sum_{g < G, i*G+g < len} in[row * len + i*G + g] for each row
+template <class F>
+__global__ void k_reduce(uint8_t* out, const uint8_t* in, int64_t rows, int64_t len, int64_t G, int64_t out_len) {
+    int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (gid >= rows * out_len) return;
+    int64_t row = gid / out_len, i = gid % out_len;
+    const Xyzz<F>* src = reinterpret_cast<const Xyzz<F>*>(in) + row * len;
+    Xyzz<F> acc;
+    set_inf(acc);
+    for (int64_t g = 0; g < G; g++) {
+        int64_t x = i * G + g;
+        if (x < len) acc = xyzz_add(acc, load_vec(src + x));
+    }
+    store_vec(reinterpret_cast<Xyzz<F>*>(out) + gid, acc);
+}
+
+template <class F>
+__global__ void k_combine(uint8_t* out, const uint8_t* wins, int64_t k, int windows, int c) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    const Xyzz<F>* W = reinterpret_cast<const Xyzz<F>*>(wins) + j * windows;
+    Xyzz<F> acc;
+    set_inf(acc);
+    for (int w = windows - 1; w >= 0; w--) {
+        if (!is_inf(acc))
+            for (int i = 0; i < c; i++) acc = xyzz_dbl(acc);
+        acc = xyzz_add(acc, load_vec(W + w));
+    }
+    store_affine(reinterpret_cast<Affine<F>*>(out + Aff<F>::SZ * j), to_affine(acc));
+}
+
+struct ScratchLayout {
+    size_t digits, entries, nnz, seg, red, total;
+};
+ScratchLayout layout_for(size_t xyzz, int32_t V, int64_t k, int64_t n, const MsmPlan& p) {
+    auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+    ScratchLayout L;
+    size_t off = 0;
+    L.digits = off;
+    off += align(sizeof(int16_t) * (size_t)V * p.windows * n);
+    L.entries = off;
+    off += align(sizeof(uint64_t) * (size_t)V * p.windows * n);
+    L.nnz = off;
+    off += align(sizeof(int32_t) * (size_t)V * p.windows);
+    L.seg = off;
+    off += align(xyzz * (size_t)k * p.windows * p.segments);
+    L.red = off;
+    size_t red_len = (size_t)((p.segments + 7) / 8);
+    off += align(xyzz * (size_t)k * p.windows * (red_len > 1 ? red_len : 1));
+    L.total = off;
+    return L;
+}
+
+template <class F>
+void run_family(uint8_t* out, const uint8_t* points, const int64_t* pbase, const int32_t* idx, const uint8_t* scalars,
+                const int32_t* vsel, int32_t V, int64_t k, int64_t n, const MsmPlan& p, uint8_t* scratch, cudaStream_t s) {
+    const size_t XZ = sizeof(Xyzz<F>);
+    ScratchLayout L = layout_for(XZ, V, k, n, p);
+    int16_t* digits = reinterpret_cast<int16_t*>(scratch + L.digits);
+    uint64_t* entries = reinterpret_cast<uint64_t*>(scratch + L.entries);
+    int32_t* nnz = reinterpret_cast<int32_t*>(scratch + L.nnz);
+    uint8_t* seg = scratch + L.seg;
+    uint8_t* red = scratch + L.red;
+    int64_t total = (int64_t)V * n;
+    note_launch();
+    k_digits<<<blocks_for(total), TPB, 0, s>>>(digits, scalars, total, n, p.c, p.windows);
+    size_t shmem = sizeof(int32_t) * 2 * (p.buckets + 1);
+    note_launch();
+    k_sort<<<(unsigned)((int64_t)V * p.windows), 256, shmem, s>>>(entries, nnz, digits, n, p.buckets);
+    int64_t segthreads = k * p.windows * p.segments;
+    note_launch();
+    k_segments<F><<<blocks_for(segthreads, 64), 64, 0, s>>>(seg, points, pbase, idx, entries, nnz, vsel, k, n,
+                                                           p.windows, p.segment, p.segments);
+    // tree-reduce segments per (MSM, window)
+    int64_t rows = k * p.windows, len = p.segments;
+    uint8_t* src = seg;
+    uint8_t* bufs[2] = {red, seg};
+    int flip = 0;
+    while (len > 1) {
+        int64_t G = len < 8 ? len : 8;
+        int64_t out_len = (len + G - 1) / G;
+        uint8_t* dst = bufs[flip];
+        note_launch();
+        k_reduce<F><<<blocks_for(rows * out_len, 64), 64, 0, s>>>(dst, src, rows, len, G, out_len);
+        src = dst;
+        flip ^= 1;
+        len = out_len;
+    }
+    note_launch();
+    k_combine<F><<<blocks_for(k, 64), 64, 0, s>>>(out, src, k, p.windows, p.c);
+}
+}  // namespace
+
+MsmPlan msm_plan(int64_t n, int64_t k) {
+    MsmPlan p;
+    int lg = 0;
+    while ((int64_t(1) << (lg + 1)) <= n) lg++;
+    int c = lg - 1;
+    if (n >= (1 << 14)) c = lg - 2;
+    if (c < 4) c = 4;
+    if (c > 13) c = 13;
+    p.c = c;
+    p.windows = (256 + c - 1) / c;
+    p.buckets = 1 << (c - 1);
+    // segment length: keep enough independent threads in flight
+    int64_t S = n;
+    int64_t want = 148 * 256;
+    while (S > 64 && k * p.windows * ((n + S - 1) / S) < want) S = (S + 1) / 2;
+    if (S < 1) S = 1;
+    p.segment = S;
+    p.segments = (n + S - 1) / S;
+    if (p.segments < 1) p.segments = 1;
+    return p;
+}
+
+size_t msm_family_scratch_bytes(Group g, int32_t V, int64_t k, int64_t n, const MsmPlan& plan) {
+    return layout_for(g == GROUP_G1 ? G1_XYZZ : G2_XYZZ, V, k, n, plan).total;
+}
+
+void launch_msm_family_scratch(Group g, uint8_t* out, const uint8_t* points, const int64_t* pbase, const int32_t* idx,
+                               const uint8_t* scalars, const int32_t* vsel, int32_t V, int64_t k, int64_t n,
+                               const MsmPlan& plan, void* scratch, cudaStream_t s) {
+    if (k <= 0) return;
+    if (g == GROUP_G1)
+        run_family<Fp>(out, points, pbase, idx, scalars, vsel, V, k, n, plan, (uint8_t*)scratch, s);
+    else
+        run_family<Fp2>(out, points, pbase, idx, scalars, vsel, V, k, n, plan, (uint8_t*)scratch, s);
+}
+
+void launch_msm_family(Group g, uint8_t* out, const uint8_t* points, const int64_t* pbase, const int32_t* idx,
+                       const uint8_t* scalars, const int32_t* vsel, int32_t V, int64_t k, int64_t n, cudaStream_t s,
+                       const MsmPlan* forced) {
+    if (k <= 0) return;
+    if (n <= 0) {
+        cudaMemsetAsync(out, 0, (g == GROUP_G1 ? G1_AFF : G2_AFF) * (size_t)k, s);
+        return;
+    }
+    MsmPlan p = forced ? *forced : msm_plan(n, k);
+    size_t bytes = msm_family_scratch_bytes(g, V, k, n, p);
+    void* scratch = nullptr;
+    if (cudaMallocAsync(&scratch, bytes, s) != cudaSuccess) return;
+    launch_msm_family_scratch(g, out, points, pbase, idx, scalars, vsel, V, k, n, p, scratch, s);
+    cudaFreeAsync(scratch, s);
+}
+
+}  // namespace wbte

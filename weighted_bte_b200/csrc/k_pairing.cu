@@ -1,0 +1,292 @@
+// Pairing-side kernels: G2 line tables, Miller loops, split final
+// exponentiation, the cyclotomic/GT radix-2 transforms and GT
+// exponentiation.
+#include "launch.h"
+#include "pairing.cuh"
+
+namespace wbte {
+
+namespace {
+constexpr int TPB = 64;
+inline unsigned blocks_for(int64_t n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+WBTE_INL Fp12* as_gt(uint8_t* p) { return reinterpret_cast<Fp12*>(p); }
+WBTE_INL const Fp12* as_gt(const uint8_t* p) { return reinterpret_cast<const Fp12*>(p); }
+
+__global__ void k_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Line* L = reinterpret_cast<Line*>(lines);
+    G2A Q = load_affine(reinterpret_cast<const G2A*>(q + G2_AFF * i));
+    if (is_inf(Q)) {
+        // identity lines: every line value is 1, so the loop returns 1
+        Line one{fp2_one(), fp2_zero(), fp2_zero()};
+        for (int s = 0; s < MILLER_LINES; s++) store_vec(L + (int64_t)s * n + i, one);
+        return;
+    }
+    G2Proj T = g2proj_from_affine(Q);
+    int idx = 0;
+    for (int b = 62; b >= 0; b--) {
+        store_vec(L + (int64_t)(idx++) * n + i, line_double(T));
+        if ((X_ABS >> b) & 1) store_vec(L + (int64_t)(idx++) * n + i, line_add(T, Q));
+    }
+}
+
+__global__ void k_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    G1A P = load_affine(reinterpret_cast<const G1A*>(p + G1_AFF * i));
+    Fp12 f;
+    miller_loop_lines(f, reinterpret_cast<const Line*>(lines) + i, (size_t)n, P);
+    store_vec(as_gt(out) + i, f);
+}
+
+__global__ void k_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, int64_t p_mod) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    G1A P = load_affine(reinterpret_cast<const G1A*>(p + G1_AFF * (p_mod ? i % p_mod : i)));
+    G2A Q = load_affine(reinterpret_cast<const G2A*>(q + G2_AFF * i));
+    Fp12 f;
+    miller_loop(f, P, Q);
+    store_vec(as_gt(out) + i, f);
+}
+
+__global__ void k_fp12_segment_product(uint8_t* out, const uint8_t* in, const int64_t* offsets, int64_t k) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    Fp12 acc = fp12_one();
+    for (int64_t t = offsets[j]; t < offsets[j + 1]; t++) {
+        Fp12 x = load_vec(as_gt(in) + t);
+        fp12_mul(acc, acc, x);
+    }
+    store_vec(as_gt(out) + j, acc);
+}
+
+__global__ void k_final_exp(uint8_t* out, const uint8_t* in, int64_t n, int mode) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fp12 f = load_vec(as_gt(in) + i), r;
+    if (mode == FE_EASY) {
+        final_exp_easy(r, f);
+    } else if (mode == FE_HARD) {
+        final_exp_hard(r, f);
+    } else {
+        final_exp_easy(r, f);
+        final_exp_hard(r, r);
+    }
+    store_vec(as_gt(out) + i, r);
+}
+
+__device__ __forceinline__ int64_t bitrev64(int64_t i, int bits) {
+    return bits ? (int64_t)(__brevll((unsigned long long)i) >> (64 - bits)) : 0;
+}
+
+__global__ void k_gt_bitrev(uint8_t* dst, const uint8_t* src, int64_t n, int bits) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    store_vec(as_gt(dst) + bitrev64(i, bits), load_vec(as_gt(src) + i));
+}
+
+// One butterfly per thread: u' = u * t, v' = u * t^-1 with t = v^tw (decomposed
+// action; inverse by conjugation in the cyclotomic subgroup).
+__global__ void k_gt_stage(uint8_t* io, const uint8_t* tw, int64_t n, int64_t half) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n / 2) return;
+    int64_t chunk = t / half, j = t % half;
+    int64_t a = chunk * 2 * half + j, b = a + half;
+    Fp12 u = load_vec(as_gt(io) + a), v = load_vec(as_gt(io) + b);
+    Fp12 tv;
+    if (j != 0) {
+        uint32_t s[8];
+        load_scalar(s, tw + FR_SZ * (j * (n / (2 * half))));
+        gt_pow(tv, v, s);
+    } else {
+        tv = v;
+    }
+    Fp12 x, y, ti;
+    fp12_mul(x, u, tv);
+    fp12_conj(ti, tv);
+    fp12_mul(y, u, ti);
+    store_vec(as_gt(io) + a, x);
+    store_vec(as_gt(io) + b, y);
+}
+
+// last stage keeping only the first out_count outputs
+__global__ void k_gt_last_prefix(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= out_count) return;
+    int64_t half = n / 2;
+    Fp12 u = load_vec(as_gt(io) + j), v = load_vec(as_gt(io) + half + j);
+    Fp12 tv;
+    if (j != 0) {
+        uint32_t s[8];
+        load_scalar(s, tw + FR_SZ * j);
+        gt_pow(tv, v, s);
+    } else {
+        tv = v;
+    }
+    fp12_mul(u, u, tv);
+    store_vec(as_gt(io) + j, u);
+}
+
+__global__ void k_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint8_t* scalars, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fp12 b = load_vec(as_gt(base) + stride * i), r;
+    uint32_t s[8];
+    load_scalar(s, scalars + FR_SZ * i);
+    gt_pow(r, b, s);
+    store_vec(as_gt(out) + i, r);
+}
+
+__global__ void k_fp12_mul(uint8_t* out, const uint8_t* a, int64_t sa, const uint8_t* b, int64_t sb, bool conj_b, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fp12 x = load_vec(as_gt(a) + sa * i), y = load_vec(as_gt(b) + sb * i), r;
+    if (conj_b) fp12_conj(y, y);
+    fp12_mul(r, x, y);
+    store_vec(as_gt(out) + i, r);
+}
+
+__global__ void k_unmask(uint8_t* out, const uint8_t* second, const uint8_t* alpha, const uint8_t* beta,
+                         const uint8_t* valid, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fp12 r;
+    if (valid[i]) {
+        Fp12 c2 = load_vec(as_gt(second) + i), al = load_vec(as_gt(alpha) + i), be = load_vec(as_gt(beta) + i);
+        fp12_conj(al, al);
+        fp12_mul(r, c2, al);
+        fp12_mul(r, r, be);
+    } else {
+        r = fp12_one();
+    }
+    store_vec(as_gt(out) + i, r);
+}
+
+WBTE_INL void fp_store_be48(uint8_t* out, const Fp& m) {
+    Fp c = fp_from_mont(m);
+    for (int i = 0; i < 48; i++) out[47 - i] = (uint8_t)(c.v[i >> 2] >> (8 * (i & 3)));
+}
+
+// Tagged torus compression of GT: identity -> 0; otherwise 1 followed by the
+// six Fp2 coefficients of (c0 + 1) / c1, each Fp as 48 big-endian bytes.
+__global__ void k_gt_compress(uint8_t* out, const uint8_t* in, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fp12 f = load_vec(as_gt(in) + i);
+    uint8_t* o = out + 289 * i;
+    if (fp12_is_one(f)) {
+        for (int b = 0; b < 289; b++) o[b] = 0;
+        return;
+    }
+    Fp6 c0 = f.c0, inv, b;
+    c0.c0 = fp2_add(c0.c0, fp2_one());
+    fp6_inv(inv, f.c1);
+    fp6_mul(b, c0, inv);
+    o[0] = 1;
+    const Fp2* cs[3] = {&b.c0, &b.c1, &b.c2};
+    for (int k = 0; k < 3; k++) {
+        fp_store_be48(o + 1 + 96 * k, cs[k]->c0);
+        fp_store_be48(o + 1 + 96 * k + 48, cs[k]->c1);
+    }
+}
+
+__global__ void k_fp12_mask(uint8_t* io, const uint8_t* valid, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!valid[i]) store_vec(as_gt(io) + i, fp12_one());
+}
+
+__global__ void k_fp12_is_one(uint8_t* flags, const uint8_t* in, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flags[i] = fp12_is_one(load_vec(as_gt(in) + i)) ? 1 : 0;
+}
+}  // namespace
+
+// ============================================================ launchers
+void launch_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_prepare_lines<<<blocks_for(n), TPB, 0, s>>>(lines, q, n);
+}
+void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_miller_lines<<<blocks_for(n), TPB, 0, s>>>(out, lines, p, n);
+}
+void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, cudaStream_t s, int64_t p_mod) {
+    if (n <= 0) return;
+    note_launch();
+    k_miller<<<blocks_for(n), TPB, 0, s>>>(out, p, q, n, p_mod);
+}
+void launch_fp12_mask(uint8_t* io, const uint8_t* valid, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_fp12_mask<<<blocks_for(n), TPB, 0, s>>>(io, valid, n);
+}
+void launch_fp12_segment_product(uint8_t* out, const uint8_t* in, const int64_t* offsets, int64_t k, cudaStream_t s) {
+    if (k <= 0) return;
+    note_launch();
+    k_fp12_segment_product<<<blocks_for(k), TPB, 0, s>>>(out, in, offsets, k);
+}
+void launch_final_exp(uint8_t* out, const uint8_t* in, int64_t n, FinalExpMode mode, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_final_exp<<<blocks_for(n), TPB, 0, s>>>(out, in, n, (int)mode);
+}
+
+static void gt_transform(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count, bool prefix, cudaStream_t s) {
+    if (n <= 1) return;
+    int bits = 0;
+    while ((int64_t(1) << bits) < n) bits++;
+    uint8_t* tmp = nullptr;
+    if (cudaMallocAsync(&tmp, GT_SZ * (size_t)n, s) != cudaSuccess) return;
+    note_launch();
+    k_gt_bitrev<<<blocks_for(n), TPB, 0, s>>>(tmp, io, n, bits);
+    int64_t last_half = prefix ? n / 4 : n / 2;
+    for (int64_t half = 1; half <= last_half; half *= 2) {
+        note_launch();
+        k_gt_stage<<<blocks_for(n / 2), TPB, 0, s>>>(tmp, tw, n, half);
+    }
+    if (prefix && out_count > 0) {
+        note_launch();
+        k_gt_last_prefix<<<blocks_for(out_count), TPB, 0, s>>>(tmp, tw, n, out_count);
+    }
+    cudaMemcpyAsync(io, tmp, GT_SZ * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    cudaFreeAsync(tmp, s);
+}
+void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* tw_inv, int64_t n, int64_t out_count, cudaStream_t s) {
+    gt_transform(io, tw_inv, n, out_count, true, s);
+}
+void launch_gt_ntt(uint8_t* io, const uint8_t* tw, int64_t n, cudaStream_t s) { gt_transform(io, tw, n, n, false, s); }
+
+void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint8_t* scalars, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_gt_pow<<<blocks_for(n), TPB, 0, s>>>(out, base, stride, scalars, n);
+}
+void launch_fp12_mul(uint8_t* out, const uint8_t* a, int64_t sa, const uint8_t* b, int64_t sb, bool conj_b, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_fp12_mul<<<blocks_for(n), TPB, 0, s>>>(out, a, sa, b, sb, conj_b, n);
+}
+void launch_unmask(uint8_t* out, const uint8_t* second, const uint8_t* alpha, const uint8_t* beta, const uint8_t* valid,
+                   int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_unmask<<<blocks_for(n), TPB, 0, s>>>(out, second, alpha, beta, valid, n);
+}
+void launch_gt_compress(uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_gt_compress<<<blocks_for(n), TPB, 0, s>>>(out, in, n);
+}
+void launch_fp12_is_one(uint8_t* flags, const uint8_t* in, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_fp12_is_one<<<blocks_for(n), TPB, 0, s>>>(flags, in, n);
+}
+
+}  // namespace wbte

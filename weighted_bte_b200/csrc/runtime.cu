@@ -1,0 +1,817 @@
+// libwbte runtime: the C ABI of include/wbte.h on top of the kernel
+// launchers.  Host or device buffers are accepted for every data pointer;
+// host buffers are staged through stream-ordered device allocations.
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "launch.h"
+#include "wbte.h"
+
+using namespace wbte;
+
+namespace wbte {
+std::atomic<uint64_t> g_launches{0};
+}
+
+struct wbte_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0;
+    std::string err;
+    std::map<std::pair<int64_t, int>, uint8_t*> twiddles;
+    std::mutex mu;
+};
+
+namespace {
+
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int log2_exact(uint64_t n) {
+    int lg = 0;
+    while ((uint64_t(1) << lg) < n) lg++;
+    return (uint64_t(1) << lg) == n ? lg : -1;
+}
+
+uint64_t next_pow2(uint64_t n) {
+    uint64_t m = 1;
+    while (m < n) m <<= 1;
+    return m;
+}
+
+// One ABI call: staging buffers, pending host copies, first error.
+struct Call {
+    wbte_ctx* ctx;
+    cudaStream_t s;
+    std::vector<void*> temps;
+    struct Pending {
+        void* host;
+        const void* dev;
+        size_t bytes;
+    };
+    std::vector<Pending> outs;
+    int32_t status = WBTE_OK;
+    bool sync = false;
+
+    explicit Call(wbte_ctx* c) : ctx(c), s(c->stream) { cudaSetDevice(c->device); }
+
+    int32_t fail(int32_t code, const std::string& msg) {
+        if (status == WBTE_OK) {
+            status = code;
+            ctx->err = msg;
+        }
+        return code;
+    }
+    bool ok() const { return status == WBTE_OK; }
+    uint8_t* alloc(size_t bytes) {
+        void* p = nullptr;
+        if (bytes == 0) bytes = 16;
+        if (cudaMallocAsync(&p, bytes, s) != cudaSuccess) {
+            cudaGetLastError();
+            fail(WBTE_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+            return nullptr;
+        }
+        temps.push_back(p);
+        return (uint8_t*)p;
+    }
+    uint8_t* zeros(size_t bytes) {
+        uint8_t* p = alloc(bytes);
+        if (p) cudaMemsetAsync(p, 0, bytes, s);
+        return p;
+    }
+    const uint8_t* in(const void* p, size_t bytes) {
+        if (!p || bytes == 0 || is_device_ptr(p)) return (const uint8_t*)p;
+        uint8_t* d = alloc(bytes);
+        if (d) cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, s);
+        return d;
+    }
+    template <class T> const T* in_vec(const std::vector<T>& v) {
+        return reinterpret_cast<const T*>(in(v.data(), v.size() * sizeof(T)));
+    }
+    uint8_t* out(void* p, size_t bytes) {
+        if (!p) return nullptr;
+        if (is_device_ptr(p)) return (uint8_t*)p;
+        uint8_t* d = alloc(bytes);
+        if (d) outs.push_back({p, d, bytes});
+        return d;
+    }
+    uint8_t* inout(void* p, size_t bytes) {
+        if (!p) return nullptr;
+        if (is_device_ptr(p)) return (uint8_t*)p;
+        uint8_t* d = alloc(bytes);
+        if (d) {
+            cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, s);
+            outs.push_back({p, d, bytes});
+        }
+        return d;
+    }
+    // copy a small device or host buffer to host (synchronising)
+    bool to_host(void* dst, const void* src, size_t bytes) {
+        if (cudaMemcpyAsync(dst, src, bytes, is_device_ptr(src) ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            fail(WBTE_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+            return false;
+        }
+        return true;
+    }
+    int32_t finish() {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) fail(WBTE_ERR_CUDA, cudaGetErrorString(e));
+        for (auto& o : outs) cudaMemcpyAsync(o.host, o.dev, o.bytes, cudaMemcpyDeviceToHost, s);
+        for (void* p : temps) cudaFreeAsync(p, s);
+        if (!outs.empty() || sync || status != WBTE_OK) {
+            e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) fail(WBTE_ERR_CUDA, cudaGetErrorString(e));
+        }
+        return status;
+    }
+};
+
+const uint8_t* twiddles(Call& c, int64_t n, bool inverse) {
+    std::lock_guard<std::mutex> lock(c.ctx->mu);
+    auto key = std::make_pair(n, inverse ? 1 : 0);
+    auto it = c.ctx->twiddles.find(key);
+    if (it != c.ctx->twiddles.end()) return it->second;
+    int64_t count = n / 2 > 0 ? n / 2 : 1;
+    uint8_t* t = nullptr;
+    if (cudaMalloc(&t, FR_SZ * count) != cudaSuccess) {
+        cudaGetLastError();
+        c.fail(WBTE_ERR_OOM, "twiddle table allocation failed");
+        return nullptr;
+    }
+    launch_domain_twiddles(t, n, count, inverse, c.s);
+    c.ctx->twiddles[key] = t;
+    return t;
+}
+
+// product of n Fp12 values on the device into out (one value)
+void fp12_product(Call& c, uint8_t* out, const uint8_t* in, int64_t n) {
+    if (n <= 0) {
+        return;
+    }
+    const int64_t G = 16;
+    const uint8_t* cur = in;
+    while (true) {
+        int64_t groups = (n + G - 1) / G;
+        std::vector<int64_t> offs(groups + 1);
+        for (int64_t j = 0; j <= groups; j++) offs[j] = std::min(n, j * G);
+        uint8_t* dst = groups == 1 ? out : c.alloc(GT_SZ * groups);
+        const int64_t* doffs = c.in_vec(offs);
+        if (!c.ok()) return;
+        launch_fp12_segment_product(dst, cur, doffs, groups, c.s);
+        if (groups == 1) return;
+        cur = dst;
+        n = groups;
+    }
+}
+
+// G2 generator affine bytes on the device
+uint8_t* g2_generator_dev(Call& c) {
+    uint8_t one[32] = {1};
+    const uint8_t* s = c.in(one, 32);
+    uint8_t* g = c.alloc(G2_AFF);
+    if (c.ok()) launch_mul_generator(GROUP_G2, g, s, 1, c.s);
+    return g;
+}
+
+int32_t check_ctx(wbte_ctx* ctx) { return ctx ? WBTE_OK : WBTE_ERR_INVALID_ARG; }
+
+int32_t msm_family_impl(wbte_ctx* ctx, Group g, void* out, const void* points, uint64_t n_points, const int64_t* pbase,
+                        const int32_t* pidx, const void* scalars, const int32_t* vsel, int32_t V, uint64_t k, uint64_t n) {
+    if (check_ctx(ctx)) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    if (k == 0) return c.finish();
+    if (!out || !pbase || V < 1 || (n > 0 && (!points || !scalars))) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    if (n >= (uint64_t(1) << 31)) return c.fail(WBTE_ERR_SIZE, "MSM length must be below 2^31");
+    // bounds: every addressed point must lie inside [0, n_points)
+    int64_t max_idx = -1, min_idx = 0;
+    if (pidx) {
+        for (uint64_t t = 0; t < n; t++) {
+            max_idx = std::max<int64_t>(max_idx, pidx[t]);
+            min_idx = std::min<int64_t>(min_idx, pidx[t]);
+        }
+    } else {
+        max_idx = (int64_t)n - 1;
+    }
+    for (uint64_t j = 0; j < k; j++) {
+        if (pbase[j] < 0 || min_idx < 0 || (n > 0 && (uint64_t)(pbase[j] + max_idx) >= n_points))
+            return c.fail(WBTE_ERR_SIZE, "MSM point index out of range");
+        if (vsel && (vsel[j] < 0 || vsel[j] >= V)) return c.fail(WBTE_ERR_INVALID_ARG, "scalar vector index out of range");
+    }
+    uint8_t* dout = c.out(out, aff * k);
+    const uint8_t* dpts = c.in(points, aff * n_points);
+    const uint8_t* dsc = c.in(scalars, FR_SZ * (size_t)V * n);
+    std::vector<int64_t> hb(pbase, pbase + k);
+    const int64_t* db = c.in_vec(hb);
+    const int32_t* di = nullptr;
+    if (pidx) {
+        std::vector<int32_t> hi(pidx, pidx + n);
+        di = c.in_vec(hi);
+    }
+    const int32_t* dv = nullptr;
+    if (vsel) {
+        std::vector<int32_t> hv(vsel, vsel + k);
+        dv = c.in_vec(hv);
+    }
+    if (!c.ok()) return c.finish();
+    launch_msm_family(g, dout, dpts, db, di, dsc, dv, V, (int64_t)k, (int64_t)n, c.s);
+    return c.finish();
+}
+
+int32_t msm_impl(wbte_ctx* ctx, Group g, void* out, const void* points, const void* scalars, uint64_t n) {
+    int64_t zero = 0;
+    return msm_family_impl(ctx, g, out, points, n, &zero, nullptr, scalars, nullptr, 1, 1, n);
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+int32_t wbte_version(void) { return 10000; }
+
+int32_t wbte_ctx_create(int32_t device, uint64_t budget, wbte_ctx** out) {
+    if (!out) return WBTE_ERR_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return WBTE_ERR_CUDA;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return WBTE_ERR_CUDA;
+    wbte_ctx* c = new wbte_ctx();
+    c->device = device;
+    c->budget = budget;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return WBTE_ERR_CUDA;
+    }
+    c->stream = c->own_stream;
+    // keep freed pool memory cached between calls
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t threshold = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    *out = c;
+    return WBTE_OK;
+}
+
+int32_t wbte_ctx_destroy(wbte_ctx* ctx) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->twiddles) cudaFree(kv.second);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return WBTE_OK;
+}
+
+int32_t wbte_ctx_set_stream(wbte_ctx* ctx, void* stream) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return WBTE_OK;
+}
+
+int32_t wbte_ctx_synchronize(wbte_ctx* ctx) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        ctx->err = cudaGetErrorString(e);
+        return WBTE_ERR_CUDA;
+    }
+    return WBTE_OK;
+}
+
+const char* wbte_ctx_last_error(const wbte_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+uint64_t wbte_ctx_launch_count(const wbte_ctx* ctx) {
+    (void)ctx;
+    return g_launches.load();
+}
+
+// ------------------------------------------------------------------ MSM
+int32_t wbte_g1_msm(wbte_ctx* ctx, void* out, const void* points, const void* scalars, uint64_t n) {
+    return msm_impl(ctx, GROUP_G1, out, points, scalars, n);
+}
+int32_t wbte_g2_msm(wbte_ctx* ctx, void* out, const void* points, const void* scalars, uint64_t n) {
+    return msm_impl(ctx, GROUP_G2, out, points, scalars, n);
+}
+int32_t wbte_g1_msm_family(wbte_ctx* ctx, void* out, const void* points, uint64_t n_points, const int64_t* pbase,
+                           const int32_t* pidx, const void* scalars, const int32_t* vsel, int32_t V, uint64_t k, uint64_t n) {
+    return msm_family_impl(ctx, GROUP_G1, out, points, n_points, pbase, pidx, scalars, vsel, V, k, n);
+}
+int32_t wbte_g2_msm_family(wbte_ctx* ctx, void* out, const void* points, uint64_t n_points, const int64_t* pbase,
+                           const int32_t* pidx, const void* scalars, const int32_t* vsel, int32_t V, uint64_t k, uint64_t n) {
+    return msm_family_impl(ctx, GROUP_G2, out, points, n_points, pbase, pidx, scalars, vsel, V, k, n);
+}
+
+// ---------------------------------------------------------- point ops
+static int32_t mul_impl(wbte_ctx* ctx, Group g, void* out, const void* points, int32_t fixed, const void* scalars, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !points || !scalars) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    uint8_t* d = c.out(out, aff * n);
+    const uint8_t* p = c.in(points, aff * (fixed ? 1 : n));
+    const uint8_t* sc = c.in(scalars, FR_SZ * n);
+    if (c.ok()) launch_mul_batch(g, d, p, fixed ? 0 : 1, sc, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_g1_mul(wbte_ctx* ctx, void* out, const void* points, int32_t fixed, const void* scalars, uint64_t n) {
+    return mul_impl(ctx, GROUP_G1, out, points, fixed, scalars, n);
+}
+int32_t wbte_g2_mul(wbte_ctx* ctx, void* out, const void* points, int32_t fixed, const void* scalars, uint64_t n) {
+    return mul_impl(ctx, GROUP_G2, out, points, fixed, scalars, n);
+}
+static int32_t mul_gen_impl(wbte_ctx* ctx, Group g, void* out, const void* scalars, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !scalars) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    uint8_t* d = c.out(out, aff * n);
+    const uint8_t* sc = c.in(scalars, FR_SZ * n);
+    if (c.ok()) launch_mul_generator(g, d, sc, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_g1_mul_generator(wbte_ctx* ctx, void* out, const void* scalars, uint64_t n) {
+    return mul_gen_impl(ctx, GROUP_G1, out, scalars, n);
+}
+int32_t wbte_g2_mul_generator(wbte_ctx* ctx, void* out, const void* scalars, uint64_t n) {
+    return mul_gen_impl(ctx, GROUP_G2, out, scalars, n);
+}
+static int32_t sum_impl(wbte_ctx* ctx, Group g, void* out, const void* in, const int64_t* offsets, uint64_t k) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (k == 0) return c.finish();
+    if (!out || !offsets) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    for (uint64_t j = 0; j < k; j++)
+        if (offsets[j + 1] < offsets[j] || offsets[0] < 0) return c.fail(WBTE_ERR_INVALID_ARG, "offsets must be ascending");
+    size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    uint8_t* d = c.out(out, aff * k);
+    const uint8_t* din = c.in(in, aff * (size_t)offsets[k]);
+    std::vector<int64_t> ho(offsets, offsets + k + 1);
+    const int64_t* doffs = c.in_vec(ho);
+    if (c.ok()) launch_segment_sum(g, d, din, doffs, (int64_t)k, c.s);
+    return c.finish();
+}
+int32_t wbte_g1_sum(wbte_ctx* ctx, void* out, const void* in, const int64_t* offsets, uint64_t k) {
+    return sum_impl(ctx, GROUP_G1, out, in, offsets, k);
+}
+int32_t wbte_g2_sum(wbte_ctx* ctx, void* out, const void* in, const int64_t* offsets, uint64_t k) {
+    return sum_impl(ctx, GROUP_G2, out, in, offsets, k);
+}
+static int32_t compress_impl(wbte_ctx* ctx, Group g, void* out, const void* in, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !in) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    uint8_t* d = c.out(out, (aff / 2) * n);
+    const uint8_t* s = c.in(in, aff * n);
+    if (c.ok()) launch_compress(g, d, s, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_g1_compress(wbte_ctx* ctx, void* out, const void* in, uint64_t n) { return compress_impl(ctx, GROUP_G1, out, in, n); }
+int32_t wbte_g2_compress(wbte_ctx* ctx, void* out, const void* in, uint64_t n) { return compress_impl(ctx, GROUP_G2, out, in, n); }
+
+// ----------------------------------------------------------- transforms
+static int32_t ntt_impl(wbte_ctx* ctx, Group g, void* io, uint64_t n, int32_t inverse) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!io) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    int lg = log2_exact(n);
+    if (n == 0 || lg < 0 || lg > 32) return c.fail(WBTE_ERR_SIZE, "transform size must be a power of two <= 2^32");
+    if (n == 1) return c.finish();
+    size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    size_t xz = g == GROUP_G1 ? G1_XYZZ : G2_XYZZ;
+    uint8_t* d = c.inout(io, aff * n);
+    uint8_t* work = c.alloc(xz * n);
+    const uint8_t* tw = twiddles(c, (int64_t)n, inverse != 0);
+    if (c.ok()) launch_group_ntt(g, d, work, tw, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_g1_ntt(wbte_ctx* ctx, void* io, uint64_t n, int32_t inverse) { return ntt_impl(ctx, GROUP_G1, io, n, inverse); }
+int32_t wbte_g2_ntt(wbte_ctx* ctx, void* io, uint64_t n, int32_t inverse) { return ntt_impl(ctx, GROUP_G2, io, n, inverse); }
+
+int32_t wbte_gt_ntt(wbte_ctx* ctx, void* io, uint64_t n, int32_t inverse) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!io) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    int lg = log2_exact(n);
+    if (n == 0 || lg < 0 || lg > 32) return c.fail(WBTE_ERR_SIZE, "transform size must be a power of two <= 2^32");
+    if (n == 1) return c.finish();
+    uint8_t* d = c.inout(io, GT_SZ * n);
+    const uint8_t* tw = twiddles(c, (int64_t)n, inverse != 0);
+    if (c.ok()) launch_gt_ntt(d, tw, (int64_t)n, c.s);
+    return c.finish();
+}
+
+int32_t wbte_gt_cyclotomic_prefix_ifft(wbte_ctx* ctx, void* io, uint64_t n, uint64_t out_count) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!io) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    int lg = log2_exact(n);
+    if (n < 2 || lg < 0 || lg > 32) return c.fail(WBTE_ERR_SIZE, "transform size must be a power of two in [2, 2^32]");
+    if (out_count > n / 2) return c.fail(WBTE_ERR_SIZE, "out_count must be at most n / 2");
+    uint8_t* d = c.inout(io, GT_SZ * n);
+    const uint8_t* tw = twiddles(c, (int64_t)n, true);
+    if (c.ok()) launch_cyclotomic_prefix_ifft(d, tw, (int64_t)n, (int64_t)out_count, c.s);
+    return c.finish();
+}
+
+// -------------------------------------------------------------- pairing
+int32_t wbte_g2_prepare_lines(wbte_ctx* ctx, void* lines, const void* q, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!lines || !q) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    uint8_t* d = c.out(lines, LINE_SZ * LINES_PER_POINT * n);
+    const uint8_t* dq = c.in(q, G2_AFF * n);
+    if (c.ok()) launch_prepare_lines(d, dq, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_miller_loop_lines(wbte_ctx* ctx, void* out, const void* lines, const void* p, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !lines || !p) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    uint8_t* d = c.out(out, GT_SZ * n);
+    const uint8_t* dl = c.in(lines, LINE_SZ * LINES_PER_POINT * n);
+    const uint8_t* dp = c.in(p, G1_AFF * n);
+    if (c.ok()) launch_miller_lines(d, dl, dp, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_miller_loop(wbte_ctx* ctx, void* out, const void* p, const void* q, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !p || !q) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    uint8_t* d = c.out(out, GT_SZ * n);
+    const uint8_t* dp = c.in(p, G1_AFF * n);
+    const uint8_t* dq = c.in(q, G2_AFF * n);
+    if (c.ok()) launch_miller(d, dp, dq, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_multi_miller_loop(wbte_ctx* ctx, void* out, const void* p, const void* q, const int64_t* offsets, uint64_t k) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (k == 0) return c.finish();
+    if (!out || !offsets) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    if (offsets[0] != 0) return c.fail(WBTE_ERR_INVALID_ARG, "offsets must start at 0");
+    for (uint64_t j = 0; j < k; j++)
+        if (offsets[j + 1] < offsets[j]) return c.fail(WBTE_ERR_INVALID_ARG, "offsets must be ascending");
+    int64_t n = offsets[k];
+    uint8_t* d = c.out(out, GT_SZ * k);
+    const uint8_t* dp = c.in(p, G1_AFF * n);
+    const uint8_t* dq = c.in(q, G2_AFF * n);
+    uint8_t* f = c.alloc(GT_SZ * (n > 0 ? n : 1));
+    std::vector<int64_t> ho(offsets, offsets + k + 1);
+    const int64_t* doffs = c.in_vec(ho);
+    if (!c.ok()) return c.finish();
+    launch_miller(f, dp, dq, n, c.s);
+    launch_fp12_segment_product(d, f, doffs, (int64_t)k, c.s);
+    return c.finish();
+}
+int32_t wbte_final_exp(wbte_ctx* ctx, void* out, const void* in, uint64_t n, int32_t mode) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !in) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    if (mode < 0 || mode > 2) return c.fail(WBTE_ERR_INVALID_ARG, "unknown final exponentiation mode");
+    uint8_t* d = c.out(out, GT_SZ * n);
+    const uint8_t* s = c.in(in, GT_SZ * n);
+    if (c.ok()) launch_final_exp(d, s, (int64_t)n, (FinalExpMode)mode, c.s);
+    return c.finish();
+}
+int32_t wbte_gt_pow(wbte_ctx* ctx, void* out, const void* base, int32_t fixed, const void* scalars, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !base || !scalars) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    uint8_t* d = c.out(out, GT_SZ * n);
+    const uint8_t* b = c.in(base, GT_SZ * (fixed ? 1 : n));
+    const uint8_t* sc = c.in(scalars, FR_SZ * n);
+    if (c.ok()) launch_gt_pow(d, b, fixed ? 0 : 1, sc, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_fp12_mul(wbte_ctx* ctx, void* out, const void* a, const void* b, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !a || !b) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    uint8_t* d = c.out(out, GT_SZ * n);
+    const uint8_t* da = c.in(a, GT_SZ * n);
+    const uint8_t* db = c.in(b, GT_SZ * n);
+    if (c.ok()) launch_fp12_mul(d, da, 1, db, 1, false, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_gt_compress(wbte_ctx* ctx, void* out, const void* in, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !in) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    uint8_t* d = c.out(out, 289 * n);
+    const uint8_t* s = c.in(in, GT_SZ * n);
+    if (c.ok()) launch_gt_compress(d, s, (int64_t)n, c.s);
+    return c.finish();
+}
+
+// -------------------------------------------------------------- scalars
+int32_t wbte_lagrange_at_zero(wbte_ctx* ctx, void* out, const void* points, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.fail(WBTE_ERR_INTERPOLATION, "the interpolation points must be nonempty and distinct");
+    if (!out || !points) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    uint8_t* d = c.out(out, FR_SZ * n);
+    const uint8_t* x = c.in(points, FR_SZ * n);
+    int32_t* status = (int32_t*)c.zeros(sizeof(int32_t));
+    if (!c.ok()) return c.finish();
+    launch_lagrange_at_zero(d, x, (int64_t)n, status, c.s);
+    int32_t st = 0;
+    if (c.to_host(&st, status, sizeof(st)) && st) c.fail(WBTE_ERR_INTERPOLATION, "the interpolation points must be nonempty and distinct");
+    return c.finish();
+}
+int32_t wbte_schnorr_verify(wbte_ctx* ctx, uint8_t* valid, const void* X, const void* R, const void* s, const void* ch, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!valid || !X || !R || !s || !ch) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    uint8_t* d = c.out(valid, n);
+    const uint8_t* dx = c.in(X, G1_AFF * n);
+    const uint8_t* dr = c.in(R, G1_AFF * n);
+    const uint8_t* ds = c.in(s, FR_SZ * n);
+    const uint8_t* dc = c.in(ch, FR_SZ * n);
+    if (c.ok()) launch_schnorr_verify(d, dx, dr, ds, dc, (int64_t)n, c.s);
+    return c.finish();
+}
+
+// --------------------------------------------------------- weighted_btx
+static int32_t check_key(Call& c, const wbte_wbtx_key* key) {
+    if (!key || !key->party_offsets || key->party_count == 0 || key->max_batch_size == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "invalid weighted-BTX key");
+    if ((uint64_t)key->party_offsets[key->party_count] != key->total_weight)
+        return c.fail(WBTE_ERR_INVALID_ARG, "party offsets do not sum to the total weight");
+    return WBTE_OK;
+}
+
+int32_t wbte_wbtx_partial_decrypt(wbte_ctx* ctx, void* sigma, const void* first, uint64_t B, const void* q, uint64_t T) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (T == 0) return c.finish();
+    if (!sigma || !first || !q || B == 0) return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    uint8_t* dsig = c.out(sigma, G1_AFF * T);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint8_t* dq = c.in(q, FR_SZ * T);
+    uint8_t* scalars = c.alloc(FR_SZ * T * B);
+    std::vector<int64_t> base(T, 0);
+    std::vector<int32_t> vsel(T);
+    for (uint64_t j = 0; j < T; j++) vsel[j] = (int32_t)j;
+    const int64_t* db = c.in_vec(base);
+    const int32_t* dv = c.in_vec(vsel);
+    if (!c.ok()) return c.finish();
+    for (uint64_t j = 0; j < T; j++) launch_fr_powers(scalars + FR_SZ * B * j, dq + FR_SZ * j, (int64_t)B, 1, c.s);
+    launch_msm_family(GROUP_G1, dsig, dfirst, db, nullptr, scalars, dv, (int32_t)T, (int64_t)T, (int64_t)B, c.s);
+    return c.finish();
+}
+
+int32_t wbte_wbtx_verify_shares(wbte_ctx* ctx, int32_t* ok, const wbte_wbtx_key* key, const void* first, const uint8_t* valid,
+                                uint64_t B, const void* sigma, const int64_t* party_indices, const void* challenges, uint64_t T) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!ok) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    *ok = 0;
+    if (check_key(c, key)) return c.finish();
+    if (T == 0) {
+        *ok = 1;
+        return c.finish();
+    }
+    if (!first || !valid || !sigma || !party_indices || !challenges) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    if (B == 0 || B > key->max_batch_size) return c.fail(WBTE_ERR_SIZE, "batch size out of range");
+    std::vector<uint8_t> hvalid(B);
+    if (!c.to_host(hvalid.data(), valid, B)) return c.finish();
+    std::vector<int32_t> slots, pidx(T);
+    for (uint64_t i = 0; i < B; i++)
+        if (hvalid[i]) slots.push_back((int32_t)i);
+    for (uint64_t j = 0; j < T; j++) {
+        if (party_indices[j] < 0 || (uint64_t)party_indices[j] >= key->party_count)
+            return c.fail(WBTE_ERR_INVALID_ARG, "invalid party index");
+        pidx[j] = (int32_t)party_indices[j];
+    }
+    int64_t nv = (int64_t)slots.size();
+    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint8_t* dsig = c.in(sigma, G1_AFF * T);
+    const uint8_t* dch = c.in(challenges, FR_SZ * T);
+    const uint8_t* dvk = c.in(key->verification_keys, G2_AFF * key->max_batch_size * key->party_count);
+    uint8_t* P = c.alloc(G1_AFF * (nv + 1));
+    uint8_t* Q = c.alloc(G2_AFF * (nv + 1));
+    uint8_t* f = c.alloc(GT_SZ * (nv + 1));
+    uint8_t* prod = c.alloc(GT_SZ);
+    uint8_t* flag = c.alloc(1);
+    std::vector<int64_t> zero(1, 0);
+    const int64_t* dzero = c.in_vec(zero);
+    std::vector<int64_t> vbase(nv > 0 ? nv : 1);
+    for (int64_t j = 0; j < nv; j++) vbase[j] = (int64_t)slots[j] * (int64_t)key->party_count;
+    const int64_t* dvbase = c.in_vec(vbase);
+    const int32_t* dpidx = c.in_vec(pidx);
+    const int32_t* dslots = nv ? c.in_vec(slots) : nullptr;
+    uint8_t* g2 = g2_generator_dev(c);
+    if (!c.ok()) return c.finish();
+    // aggregate sigma, negated, as the last left input
+    launch_msm_family(GROUP_G1, P + G1_AFF * nv, dsig, dzero, nullptr, dch, nullptr, 1, 1, (int64_t)T, c.s);
+    launch_negate(GROUP_G1, P + G1_AFF * nv, P + G1_AFF * nv, 1, c.s);
+    if (nv > 0) {
+        launch_gather(P, dfirst, dslots, nv, G1_AFF, c.s);
+        launch_msm_family(GROUP_G2, Q, dvk, dvbase, dpidx, dch, nullptr, 1, nv, (int64_t)T, c.s);
+    }
+    cudaMemcpyAsync(Q + G2_AFF * nv, g2, G2_AFF, cudaMemcpyDeviceToDevice, c.s);
+    launch_miller(f, P, Q, nv + 1, c.s);
+    fp12_product(c, prod, f, nv + 1);
+    launch_final_exp(prod, prod, 1, FE_FULL, c.s);
+    launch_fp12_is_one(flag, prod, 1, c.s);
+    uint8_t h = 0;
+    if (c.to_host(&h, flag, 1)) *ok = h ? 1 : 0;
+    return c.finish();
+}
+
+int32_t wbte_wbtx_prepare(wbte_ctx* ctx, const wbte_wbtx_key* key, const int64_t* party_indices, uint64_t T, uint64_t B,
+                          void* kernel_lines, void* opening_keys, void* kernel) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (check_key(c, key)) return c.finish();
+    if (!party_indices || T == 0 || !kernel_lines || !opening_keys) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    if (B == 0 || B > key->max_batch_size) return c.fail(WBTE_ERR_SIZE, "batch size out of range");
+    const uint64_t N = key->party_count, W = key->total_weight, L = key->max_batch_size;
+    const uint64_t m = next_pow2(2 * B);
+    const int lgm = log2_exact(m);
+    // accepted virtual indices and per-party coefficient offsets
+    std::vector<int32_t> sel;
+    std::vector<int64_t> coef_off(1, 0), party_base(T);
+    for (uint64_t k = 0; k < T; k++) {
+        int64_t j = party_indices[k];
+        if (j < 0 || (uint64_t)j >= N) return c.fail(WBTE_ERR_INVALID_ARG, "invalid party index");
+        if (k && party_indices[k - 1] >= j) return c.fail(WBTE_ERR_INVALID_ARG, "party indices must be strictly ascending");
+        for (int64_t w = key->party_offsets[j]; w < key->party_offsets[j + 1]; w++) sel.push_back((int32_t)w);
+        coef_off.push_back((int64_t)sel.size());
+        party_base[k] = key->party_offsets[j];
+    }
+    const int64_t WT = (int64_t)sel.size();
+    uint8_t* dlines = c.out(kernel_lines, LINE_SZ * LINES_PER_POINT * m);
+    uint8_t* dopen = c.out(opening_keys, G2_AFF * B * T);
+    uint8_t* dkern_out = kernel ? c.out(kernel, G2_AFF * m) : nullptr;
+    const uint8_t* ddom = c.in(key->domain_points, FR_SZ * W);
+    const uint8_t* dneg = c.in(key->negative_material, G2_AFF * L * W);
+    const uint8_t* dpos = L > 1 ? c.in(key->positive_material, G2_AFF * (L - 1) * W) : nullptr;
+    const int32_t* dsel = c.in_vec(sel);
+    uint8_t* x = c.alloc(FR_SZ * WT);
+    uint8_t* lam = c.alloc(FR_SZ * WT);
+    int32_t* status = (int32_t*)c.zeros(sizeof(int32_t));
+    uint8_t* kern = c.zeros(G2_AFF * m);
+    uint8_t* open_scaled = c.alloc(G2_AFF * B * T);
+    uint8_t* tmp = c.alloc(G2_AFF * B);
+    uint8_t* work = c.alloc(G2_XYZZ * m);
+    if (!c.ok()) return c.finish();
+    // Lagrange coefficients of the accepted virtual points, scaled by 1/m so
+    // that every MSM below already carries the inverse-transform factor.
+    launch_gather(x, ddom, dsel, WT, FR_SZ, c.s);
+    launch_lagrange_at_zero(lam, x, WT, status, c.s);
+    launch_fr_scale_size_inv(lam, lam, lgm, WT, c.s);
+    // A'[slot, k] = sum_{w in party k} lam'_w * negative[slot][w]
+    std::vector<int64_t> slot_base(B);
+    for (uint64_t k = 0; k < T; k++) {
+        for (uint64_t i = 0; i < B; i++) slot_base[i] = (int64_t)(i * W) + party_base[k];
+        const int64_t* dbase = c.in_vec(slot_base);
+        if (!c.ok()) return c.finish();
+        int64_t wk = coef_off[k + 1] - coef_off[k];
+        launch_msm_family(GROUP_G2, tmp, dneg, dbase, nullptr, lam + FR_SZ * coef_off[k], nullptr, 1, (int64_t)B, wk, c.s);
+        cudaMemcpy2DAsync(open_scaled + G2_AFF * k, G2_AFF * T, tmp, G2_AFF, G2_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    }
+    // kernel[d] = sum_k A'[d - 1, k] for 1 <= d < B
+    if (B > 1) {
+        std::vector<int64_t> offs(B);
+        for (uint64_t d = 0; d < B; d++) offs[d] = (int64_t)(d * T);
+        const int64_t* doffs = c.in_vec(offs);
+        if (!c.ok()) return c.finish();
+        launch_segment_sum(GROUP_G2, kern + G2_AFF, open_scaled, doffs, (int64_t)B - 1, c.s);
+        // kernel[m - d] = sum_w lam'_w positive[d - 1][sel[w]], written in ascending m - d order
+        std::vector<int64_t> pbase(B - 1);
+        for (uint64_t j = 0; j + 1 < B; j++) pbase[j] = (int64_t)((B - 2 - j) * W);
+        const int64_t* dpb = c.in_vec(pbase);
+        if (!c.ok()) return c.finish();
+        launch_msm_family(GROUP_G2, kern + G2_AFF * (m - B + 1), dpos, dpb, dsel, lam, nullptr, 1, (int64_t)B - 1, WT, c.s);
+    }
+    const uint8_t* tw = twiddles(c, (int64_t)m, false);
+    if (!c.ok()) return c.finish();
+    launch_group_ntt(GROUP_G2, kern, work, tw, (int64_t)m, c.s);
+    launch_prepare_lines(dlines, kern, (int64_t)m, c.s);
+    if (dkern_out) cudaMemcpyAsync(dkern_out, kern, G2_AFF * m, cudaMemcpyDeviceToDevice, c.s);
+    // opening keys A = m * A'
+    launch_mul_pow2(GROUP_G2, dopen, open_scaled, (int64_t)(B * T), lgm, c.s);
+    int32_t st = 0;
+    if (c.to_host(&st, status, sizeof(st)) && st) c.fail(WBTE_ERR_INTERPOLATION, "the interpolation points must be nonempty and distinct");
+    return c.finish();
+}
+
+int32_t wbte_wbtx_precompute(wbte_ctx* ctx, void* beta, const void* kernel_lines, const void* first, const uint8_t* valid, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!beta || !kernel_lines || !first || !valid || B == 0) return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    const uint64_t m = next_pow2(2 * B);
+    uint8_t* dbeta = c.out(beta, GT_SZ * B);
+    const uint8_t* dl = c.in(kernel_lines, LINE_SZ * LINES_PER_POINT * m);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint8_t* dvalid = c.in(valid, B);
+    uint8_t* x = c.zeros(G1_AFF * m);
+    uint8_t* work = c.alloc(G1_XYZZ * m);
+    uint8_t* f = c.alloc(GT_SZ * m);
+    const uint8_t* tw = twiddles(c, (int64_t)m, false);
+    const uint8_t* twi = twiddles(c, (int64_t)m, true);
+    if (!c.ok()) return c.finish();
+    cudaMemcpyAsync(x, dfirst, G1_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    launch_group_ntt(GROUP_G1, x, work, tw, (int64_t)m, c.s);
+    launch_miller_lines(f, dl, x, (int64_t)m, c.s);
+    launch_final_exp(f, f, (int64_t)m, FE_EASY, c.s);
+    launch_cyclotomic_prefix_ifft(f, twi, (int64_t)m, (int64_t)B, c.s);
+    launch_final_exp(dbeta, f, (int64_t)B, FE_HARD, c.s);
+    launch_fp12_mask(dbeta, dvalid, (int64_t)B, c.s);
+    return c.finish();
+}
+
+int32_t wbte_wbtx_open(wbte_ctx* ctx, void* messages, const void* opening_keys, const void* sigma, uint64_t T,
+                       const void* second, const void* beta, const uint8_t* valid, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!messages || !opening_keys || !sigma || !second || !beta || !valid || B == 0 || T == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    uint8_t* dm = c.out(messages, GT_SZ * B);
+    const uint8_t* dk = c.in(opening_keys, G2_AFF * B * T);
+    const uint8_t* ds = c.in(sigma, G1_AFF * T);
+    const uint8_t* d2 = c.in(second, GT_SZ * B);
+    const uint8_t* db = c.in(beta, GT_SZ * B);
+    const uint8_t* dv = c.in(valid, B);
+    uint8_t* f = c.alloc(GT_SZ * B * T);
+    uint8_t* alpha = c.alloc(GT_SZ * B);
+    std::vector<int64_t> offs(B + 1);
+    for (uint64_t i = 0; i <= B; i++) offs[i] = (int64_t)(i * T);
+    const int64_t* doffs = c.in_vec(offs);
+    if (!c.ok()) return c.finish();
+    launch_miller(f, ds, dk, (int64_t)(B * T), c.s, (int64_t)T);
+    launch_fp12_segment_product(alpha, f, doffs, (int64_t)B, c.s);
+    launch_final_exp(alpha, alpha, (int64_t)B, FE_FULL, c.s);
+    launch_unmask(dm, d2, alpha, db, dv, (int64_t)B, c.s);
+    return c.finish();
+}
+
+int32_t wbte_wbtx_keygen_material(wbte_ctx* ctx, const void* z, const int32_t* owner, const void* q_pos, const void* q_neg,
+                                  uint64_t W, uint64_t N, uint64_t L, void* vk, void* negative, void* positive) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!z || !owner || !q_pos || !q_neg || !vk || !negative || (L > 1 && !positive) || W == 0 || N == 0 || L == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty dimension");
+    for (uint64_t w = 0; w < W; w++)
+        if (owner[w] < 0 || (uint64_t)owner[w] >= N) return c.fail(WBTE_ERR_INVALID_ARG, "owner index out of range");
+    uint8_t* dvk = c.out(vk, G2_AFF * L * N);
+    uint8_t* dneg = c.out(negative, G2_AFF * L * W);
+    uint8_t* dpos = L > 1 ? c.out(positive, G2_AFF * (L - 1) * W) : nullptr;
+    const uint8_t* dz = c.in(z, FR_SZ * W);
+    const uint8_t* dqp = c.in(q_pos, FR_SZ * L * N);
+    const uint8_t* dqn = c.in(q_neg, FR_SZ * L * N);
+    std::vector<int32_t> ho(owner, owner + W);
+    const int32_t* downer = c.in_vec(ho);
+    const uint64_t rows_per_chunk = std::max<uint64_t>(1, (uint64_t(1) << 20) / W);
+    uint8_t* sc = c.alloc(FR_SZ * W * std::min<uint64_t>(rows_per_chunk, L));
+    if (!c.ok()) return c.finish();
+    launch_mul_generator(GROUP_G2, dvk, dqp, (int64_t)(L * N), c.s);
+    for (int pass = 0; pass < 2; pass++) {
+        uint64_t rows = pass == 0 ? L : L - 1;
+        const uint8_t* qp = pass == 0 ? dqn : dqp;
+        uint8_t* dst = pass == 0 ? dneg : dpos;
+        for (uint64_t r0 = 0; r0 < rows; r0 += rows_per_chunk) {
+            uint64_t nr = std::min(rows_per_chunk, rows - r0);
+            launch_material_scalars(sc, dz, downer, qp + FR_SZ * r0 * N, (int64_t)W, (int64_t)N, (int64_t)nr, c.s);
+            launch_mul_generator(GROUP_G2, dst + G2_AFF * r0 * W, sc, (int64_t)(nr * W), c.s);
+        }
+    }
+    return c.finish();
+}
+
+}  // extern "C"
