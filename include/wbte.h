@@ -62,8 +62,20 @@ int32_t wbte_ctx_destroy(wbte_ctx *ctx);
 int32_t wbte_ctx_set_stream(wbte_ctx *ctx, void *cuda_stream);
 int32_t wbte_ctx_synchronize(wbte_ctx *ctx);
 const char *wbte_ctx_last_error(const wbte_ctx *ctx);
-/* Number of kernels the context has launched so far. */
+/* Number of kernels the library has launched so far (all contexts). */
 uint64_t wbte_ctx_launch_count(const wbte_ctx *ctx);
+/* Per-kernel timing.  While enabled, every kernel launch is bracketed by CUDA
+ * events on its stream; enabling (or disabling) clears the records.
+ * wbte_profile_read synchronises the device and returns, per kernel name,
+ * the summed milliseconds and the number of launches (names are written as
+ * NUL-terminated strings name_stride bytes apart). */
+int32_t wbte_profile_enable(int32_t on);
+/* Measures the sustained rate of 32-bit integer multiply-add instructions
+ * (mad.lo/mad.hi) on the context's GPU with a calibration kernel; the
+ * denominator of the integer-pipe roofline.  Synchronous. */
+int32_t wbte_measure_imad_rate(wbte_ctx *ctx, double *imad_per_s);
+int32_t wbte_profile_read(char *names, int32_t name_stride, double *ms, int64_t *counts,
+                          int32_t max_entries, int32_t *n_out);
 
 /* --------------------------------------------------------------- MSM */
 /* Replaces blst_p1s_mult_pippenger with nbits = 255, one contiguous block

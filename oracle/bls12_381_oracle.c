@@ -1443,3 +1443,78 @@ void orc_miller_loop_projective_check(u8 *out, const u8 *g1, const u8 *g2) {
     }
     fp12_conj((fp12 *)out, &f);
 }
+
+/* Tagged torus encoding of GT (append_gt, weighted_btx/src/encoding.rs:11-19):
+ * identity -> 0 followed by zeros; else 1 followed by the Fp2 coefficients of
+ * (c0 + 1) / c1, each Fp as 48 big-endian bytes (289 bytes in total). */
+void orc_gt_compress(u8 *out289, const u8 *in576) {
+    const fp12 *f = (const fp12 *)in576;
+    memset(out289, 0, 289);
+    if (fp12_eq(f, &FP12_ONE)) return;
+    fp6 c0 = f->c0, inv, b;
+    fp2_add(&c0.c0, &c0.c0, &FP2_ONE);
+    fp6_inv(&inv, &f->c1);
+    fp6_mul(&b, &c0, &inv);
+    out289[0] = 1;
+    const fp2 *cs[3] = {&b.c0, &b.c1, &b.c2};
+    for (int k = 0; k < 3; k++) {
+        fp_to_be48(out289 + 1 + 96 * k, &cs[k]->c0);
+        fp_to_be48(out289 + 1 + 96 * k + 48, &cs[k]->c1);
+    }
+}
+
+/* Fixed-base multiples of the generators with an 8-bit comb:
+ * T[w][d] = d * 2^(8w) * G, so [s]G is the sum of T[w][byte w of s]. */
+static g1j *G1_TAB = NULL;
+static g2j *G2_TAB = NULL;
+static void build_tables(void) {
+#pragma omp critical(orc_tables)
+    {
+        if (!G1_TAB) {
+            g1j *t1 = malloc(sizeof(g1j) * 32 * 256);
+            g2j *t2 = malloc(sizeof(g2j) * 32 * 256);
+            g1j b1;
+            g2j b2;
+            g1_from_affine(&b1, &G1_GEN);
+            g2_from_affine(&b2, &G2_GEN);
+            for (int w = 0; w < 32; w++) {
+                memset(&t1[256 * w], 0, sizeof(g1j));
+                memset(&t2[256 * w], 0, sizeof(g2j));
+                for (int d = 1; d < 256; d++) {
+                    g1_add(&t1[256 * w + d], &t1[256 * w + d - 1], &b1);
+                    g2_add(&t2[256 * w + d], &t2[256 * w + d - 1], &b2);
+                }
+                for (int i = 0; i < 8; i++) {
+                    g1_dbl(&b1, &b1);
+                    g2_dbl(&b2, &b2);
+                }
+            }
+            G2_TAB = t2;
+            G1_TAB = t1;
+        }
+    }
+}
+void orc_g1_mul_generator_batch(u8 *out, const u8 *scalars, int64_t n) {
+    build_tables();
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; i++) {
+        g1j acc;
+        memset(&acc, 0, sizeof acc);
+        const u8 *s = scalars + 32 * i;
+        for (int w = 0; w < 32; w++)
+            if (s[w]) g1_add(&acc, &acc, &G1_TAB[256 * w + s[w]]);
+        g1_to_affine(G1A(out + 96 * i), &acc);
+    }
+}
+void orc_g2_mul_generator_batch(u8 *out, const u8 *scalars, int64_t n) {
+    build_tables();
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; i++) {
+        g2j acc;
+        memset(&acc, 0, sizeof acc);
+        const u8 *s = scalars + 32 * i;
+        for (int w = 0; w < 32; w++)
+            if (s[w]) g2_add(&acc, &acc, &G2_TAB[256 * w + s[w]]);
+        g2_to_affine(G2A(out + 192 * i), &acc);
+    }
+}

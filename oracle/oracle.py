@@ -408,3 +408,28 @@ def domain_generator(n: int, inverse: bool = False) -> int:
     for _ in range(lg, 32):
         g = g * g % R
     return pow(g, R - 2, R) if inverse else g
+
+
+def gt_compress(a: bytes) -> bytes:
+    o = _buf(289)
+    lib().orc_gt_compress(o, a)
+    return o.raw
+
+
+def append_gt(a: bytes) -> bytes:
+    """Tagged GT encoding: b'\\x00' for the identity, else b'\\x01' + 288 bytes."""
+    c = gt_compress(a)
+    return c[:1] if c[0] == 0 else c
+
+
+def g1_mul_generator_many(scalars) -> list:
+    n = len(scalars)
+    o = _buf(96 * max(1, n))
+    lib().orc_g1_mul_generator_batch(o, scalars_bytes(scalars), ctypes.c_int64(n))
+    return [o.raw[96 * i : 96 * (i + 1)] for i in range(n)]
+
+
+def g2_mul_generator_blob(scalar_blob: bytes, n: int) -> bytes:
+    o = _buf(192 * max(1, n))
+    lib().orc_g2_mul_generator_batch(o, scalar_blob, ctypes.c_int64(n))
+    return o.raw[: 192 * n]

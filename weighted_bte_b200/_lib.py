@@ -91,12 +91,36 @@ _SIGNATURES = {
     "wbte_wbtx_precompute": [_VP, _VP, _VP, _VP, _U64],
     "wbte_wbtx_open": [_VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64],
     "wbte_wbtx_keygen_material": [_VP, _VP, _VP, _VP, _U64, _U64, _U64, _VP, _VP, _VP],
+    "wbte_measure_imad_rate": [_VP],
 }
 EXPORTED = sorted(
     list(_SIGNATURES)
     + ["wbte_version", "wbte_ctx_create", "wbte_ctx_destroy", "wbte_ctx_set_stream", "wbte_ctx_synchronize",
-       "wbte_ctx_last_error", "wbte_ctx_launch_count"]
+       "wbte_ctx_last_error", "wbte_ctx_launch_count", "wbte_profile_enable", "wbte_profile_read"]
 )
+
+
+def profile_enable(on: bool = True) -> None:
+    """Start (or stop) per-kernel CUDA-event timing; clears earlier records."""
+    load().wbte_profile_enable(1 if on else 0)
+
+
+def profile_read() -> dict:
+    """{kernel name: (milliseconds summed over launches, launches)}."""
+    lib = load()
+    stride, cap = 64, 256
+    names = ctypes.create_string_buffer(stride * cap)
+    ms = (ctypes.c_double * cap)()
+    cnt = (ctypes.c_int64 * cap)()
+    n = _I32(0)
+    st = lib.wbte_profile_read(names, stride, ms, cnt, cap, ctypes.byref(n))
+    if st != WBTE_OK:
+        raise WbteError(st, "profile read failed")
+    out = {}
+    for i in range(n.value):
+        name = names.raw[i * stride : (i + 1) * stride].split(b"\0", 1)[0].decode()
+        out[name] = (float(ms[i]), int(cnt[i]))
+    return out
 
 _lib = None
 _lock = threading.Lock()
@@ -127,6 +151,10 @@ def load():
         lib.wbte_ctx_last_error.restype = ctypes.c_char_p
         lib.wbte_ctx_launch_count.argtypes = [_VP]
         lib.wbte_ctx_launch_count.restype = _U64
+        lib.wbte_profile_enable.argtypes = [_I32]
+        lib.wbte_profile_enable.restype = _I32
+        lib.wbte_profile_read.argtypes = [_VP, _I32, _VP, _VP, _I32, ctypes.POINTER(_I32)]
+        lib.wbte_profile_read.restype = _I32
         for name, args in _SIGNATURES.items():
             fn = getattr(lib, name)
             fn.argtypes = [_VP] + args

@@ -282,10 +282,54 @@ __global__ void k_schnorr_verify(uint8_t* valid, const uint8_t* X, const uint8_t
     valid[i] = is_inf(diff) ? 1 : 0;
 }
 
+// Integer-pipe calibration: eight independent chains of 32-bit multiply-adds
+// per thread, half low and half high products (the mix of the CIOS kernel).
+__global__ void k_imad_probe(uint32_t* sink, int iters) {
+    uint32_t a[8], b = 0x9e3779b9u + threadIdx.x;
+    for (int k = 0; k < 8; k++) a[k] = threadIdx.x * 7u + blockIdx.x + (uint32_t)k;
+    for (int i = 0; i < iters; i++) {
+        _Pragma("unroll") for (int k = 0; k < 8; k += 2) {
+            asm volatile("mad.lo.u32 %0, %0, %1, %0;" : "+r"(a[k]) : "r"(b));
+            asm volatile("mad.hi.u32 %0, %0, %1, %0;" : "+r"(a[k + 1]) : "r"(b));
+        }
+    }
+    uint32_t x = 0;
+    for (int k = 0; k < 8; k++) x ^= a[k];
+    if (x == 0x12345678u) sink[0] = x;
+}
+
 }  // namespace
+
+// IMAD instructions per second sustained by the integer pipe (measured).
+double measure_imad_rate(cudaStream_t s) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    uint32_t* sink = nullptr;
+    if (cudaMallocAsync(&sink, 16, s) != cudaSuccess) return 0.0;
+    const int iters = 8192, threads = 256, blocks = sms * 8;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    note_launch();
+    k_imad_probe<<<blocks, threads, 0, s>>>(sink, iters / 8);  // warm-up
+    cudaEventRecord(a, s);
+    note_launch();
+    k_imad_probe<<<blocks, threads, 0, s>>>(sink, iters);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFreeAsync(sink, s);
+    double ops = (double)blocks * threads * iters * 8.0;
+    return ms > 0 ? ops / (ms * 1e-3) : 0.0;
+}
 
 // ============================================================ launchers
 void launch_fr_powers(uint8_t* out, const uint8_t* base, int64_t n, int64_t first, cudaStream_t s) {
+    ProfScope prof_("fr_scalars", s);
     if (n <= 0) return;
     note_launch();
     k_fr_powers<<<blocks_for(n), TPB, 0, s>>>(out, base, n, first);
@@ -307,6 +351,7 @@ void launch_fr_scale_size_inv(uint8_t* out, const uint8_t* a, int log_m, int64_t
 }
 void launch_material_scalars(uint8_t* out, const uint8_t* z, const int32_t* owner, const uint8_t* qp, int64_t W,
                              int64_t N, int64_t rows, cudaStream_t s) {
+    ProfScope prof_("fr_scalars", s);
     if (rows * W <= 0) return;
     note_launch();
     k_material_scalars<<<blocks_for(rows * W), TPB, 0, s>>>(out, z, owner, qp, W, N, rows);
@@ -317,6 +362,7 @@ void launch_gather(uint8_t* out, const uint8_t* in, const int32_t* idx, int64_t 
     k_gather<<<blocks_for(n), TPB, 0, s>>>(out, in, idx, n, record);
 }
 void launch_lagrange_at_zero(uint8_t* out, const uint8_t* x, int64_t n, int32_t* status, cudaStream_t s) {
+    ProfScope prof_("lagrange", s);
     if (n <= 0) return;
     note_launch();
     k_lagrange<<<blocks_for(n, 64), 64, 0, s>>>(out, x, n, status);
@@ -330,6 +376,7 @@ void launch_domain_twiddles(uint8_t* tw, int64_t n, int64_t count, bool inverse,
 }
 
 void launch_mul_batch(Group g, uint8_t* out, const uint8_t* pts, int64_t stride, const uint8_t* scalars, int64_t n, cudaStream_t s) {
+    ProfScope prof_("mul_batch", s);
     if (n <= 0) return;
     note_launch();
     if (g == GROUP_G1) k_mul_batch<Fp><<<blocks_for(n), TPB, 0, s>>>(out, pts, stride, scalars, n);
@@ -339,6 +386,7 @@ void launch_mul_batch(Group g, uint8_t* out, const uint8_t* pts, int64_t stride,
 // generator tables are built once per device on first use
 static uint8_t* g_gen_table[2][64] = {};
 void launch_mul_generator(Group g, uint8_t* out, const uint8_t* scalars, int64_t n, cudaStream_t s) {
+    ProfScope prof_("mul_generator", s);
     if (n <= 0) return;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -358,12 +406,14 @@ void launch_mul_generator(Group g, uint8_t* out, const uint8_t* scalars, int64_t
 }
 
 void launch_mul_pow2(Group g, uint8_t* out, const uint8_t* in, int64_t n, int k, cudaStream_t s) {
+    ProfScope prof_("mul_pow2", s);
     if (n <= 0) return;
     note_launch();
     if (g == GROUP_G1) k_mul_pow2<Fp><<<blocks_for(n), TPB, 0, s>>>(out, in, n, k);
     else k_mul_pow2<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, in, n, k);
 }
 void launch_segment_sum(Group g, uint8_t* out, const uint8_t* in, const int64_t* offsets, int64_t k, cudaStream_t s) {
+    ProfScope prof_("point_sum", s);
     if (k <= 0) return;
     note_launch();
     if (g == GROUP_G1) k_segment_sum<Fp><<<blocks_for(k), TPB, 0, s>>>(out, in, offsets, k);
@@ -377,6 +427,7 @@ void launch_negate(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStre
 }
 
 void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, int64_t n, cudaStream_t s) {
+    ProfScope prof_(g == GROUP_G1 ? "ntt_g1" : "ntt_g2", s);
     if (n <= 0) return;
     int bits = 0;
     while ((int64_t(1) << bits) < n) bits++;
@@ -402,6 +453,7 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
 }
 
 void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {
+    ProfScope prof_("compress", s);
     if (n <= 0) return;
     note_launch();
     if (g == GROUP_G1) k_g1_compress<<<blocks_for(n), TPB, 0, s>>>(out, in, n);
@@ -410,6 +462,7 @@ void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaSt
 
 void launch_schnorr_verify(uint8_t* valid, const uint8_t* X, const uint8_t* R, const uint8_t* sresp, const uint8_t* c,
                            int64_t n, cudaStream_t st) {
+    ProfScope prof_("schnorr_verify", st);
     if (n <= 0) return;
     note_launch();
     k_schnorr_verify<<<blocks_for(n), TPB, 0, st>>>(valid, X, R, sresp, c, n);

@@ -217,15 +217,22 @@ void run_family(uint8_t* out, const uint8_t* points, const int64_t* pbase, const
     uint8_t* seg = scratch + L.seg;
     uint8_t* red = scratch + L.red;
     int64_t total = (int64_t)V * n;
+    const bool g1 = sizeof(F) == sizeof(Fp);
+    void* tok = nullptr;
+    prof_begin(g1 ? "msm_sort_g1" : "msm_sort_g2", s, &tok);
     note_launch();
     k_digits<<<blocks_for(total), TPB, 0, s>>>(digits, scalars, total, n, p.c, p.windows);
     size_t shmem = sizeof(int32_t) * 2 * (p.buckets + 1);
     note_launch();
     k_sort<<<(unsigned)((int64_t)V * p.windows), 256, shmem, s>>>(entries, nnz, digits, n, p.buckets);
+    prof_end(tok, s);
+    prof_begin(g1 ? "msm_segments_g1" : "msm_segments_g2", s, &tok);
     int64_t segthreads = k * p.windows * p.segments;
     note_launch();
     k_segments<F><<<blocks_for(segthreads, 64), 64, 0, s>>>(seg, points, pbase, idx, entries, nnz, vsel, k, n,
                                                            p.windows, p.segment, p.segments);
+    prof_end(tok, s);
+    prof_begin(g1 ? "msm_reduce_g1" : "msm_reduce_g2", s, &tok);
     // tree-reduce segments per (MSM, window)
     int64_t rows = k * p.windows, len = p.segments;
     uint8_t* src = seg;
@@ -243,6 +250,7 @@ void run_family(uint8_t* out, const uint8_t* points, const int64_t* pbase, const
     }
     note_launch();
     k_combine<F><<<blocks_for(k, 64), 64, 0, s>>>(out, src, k, p.windows, p.c);
+    prof_end(tok, s);
 }
 }  // namespace
 

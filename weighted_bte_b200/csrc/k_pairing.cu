@@ -207,16 +207,19 @@ __global__ void k_fp12_is_one(uint8_t* flags, const uint8_t* in, int64_t n) {
 
 // ============================================================ launchers
 void launch_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n, cudaStream_t s) {
+    ProfScope prof_("prepare_lines", s);
     if (n <= 0) return;
     note_launch();
     k_prepare_lines<<<blocks_for(n), TPB, 0, s>>>(lines, q, n);
 }
 void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, cudaStream_t s) {
+    ProfScope prof_("miller_lines", s);
     if (n <= 0) return;
     note_launch();
     k_miller_lines<<<blocks_for(n), TPB, 0, s>>>(out, lines, p, n);
 }
 void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, cudaStream_t s, int64_t p_mod) {
+    ProfScope prof_("miller", s);
     if (n <= 0) return;
     note_launch();
     k_miller<<<blocks_for(n), TPB, 0, s>>>(out, p, q, n, p_mod);
@@ -227,17 +230,20 @@ void launch_fp12_mask(uint8_t* io, const uint8_t* valid, int64_t n, cudaStream_t
     k_fp12_mask<<<blocks_for(n), TPB, 0, s>>>(io, valid, n);
 }
 void launch_fp12_segment_product(uint8_t* out, const uint8_t* in, const int64_t* offsets, int64_t k, cudaStream_t s) {
+    ProfScope prof_("fp12_product", s);
     if (k <= 0) return;
     note_launch();
     k_fp12_segment_product<<<blocks_for(k), TPB, 0, s>>>(out, in, offsets, k);
 }
 void launch_final_exp(uint8_t* out, const uint8_t* in, int64_t n, FinalExpMode mode, cudaStream_t s) {
+    ProfScope prof_(mode == FE_EASY ? "final_exp_easy" : (mode == FE_HARD ? "final_exp_hard" : "final_exp"), s);
     if (n <= 0) return;
     note_launch();
     k_final_exp<<<blocks_for(n), TPB, 0, s>>>(out, in, n, (int)mode);
 }
 
 static void gt_transform(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count, bool prefix, cudaStream_t s) {
+    ProfScope prof_("gt_ifft", s);
     if (n <= 1) return;
     int bits = 0;
     while ((int64_t(1) << bits) < n) bits++;
@@ -263,6 +269,7 @@ void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* tw_inv, int64_t n
 void launch_gt_ntt(uint8_t* io, const uint8_t* tw, int64_t n, cudaStream_t s) { gt_transform(io, tw, n, n, false, s); }
 
 void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint8_t* scalars, int64_t n, cudaStream_t s) {
+    ProfScope prof_("gt_pow", s);
     if (n <= 0) return;
     note_launch();
     k_gt_pow<<<blocks_for(n), TPB, 0, s>>>(out, base, stride, scalars, n);
@@ -274,11 +281,13 @@ void launch_fp12_mul(uint8_t* out, const uint8_t* a, int64_t sa, const uint8_t* 
 }
 void launch_unmask(uint8_t* out, const uint8_t* second, const uint8_t* alpha, const uint8_t* beta, const uint8_t* valid,
                    int64_t n, cudaStream_t s) {
+    ProfScope prof_("unmask", s);
     if (n <= 0) return;
     note_launch();
     k_unmask<<<blocks_for(n), TPB, 0, s>>>(out, second, alpha, beta, valid, n);
 }
 void launch_gt_compress(uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {
+    ProfScope prof_("gt_compress", s);
     if (n <= 0) return;
     note_launch();
     k_gt_compress<<<blocks_for(n), TPB, 0, s>>>(out, in, n);

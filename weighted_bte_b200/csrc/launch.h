@@ -15,6 +15,17 @@ namespace wbte {
 extern std::atomic<uint64_t> g_launches;
 inline void note_launch(uint64_t k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
+// Optional per-kernel timing: while profiling is enabled, a ProfScope records
+// CUDA events around the launches in its scope, tagged with a kernel name.
+void prof_begin(const char* tag, cudaStream_t s, void** token);
+void prof_end(void* token, cudaStream_t s);
+struct ProfScope {
+    void* token = nullptr;
+    cudaStream_t s;
+    ProfScope(const char* tag, cudaStream_t st) : s(st) { prof_begin(tag, st, &token); }
+    ~ProfScope() { prof_end(token, s); }
+};
+
 constexpr size_t G1_AFF = 96, G2_AFF = 192, G1_XYZZ = 192, G2_XYZZ = 384, GT_SZ = 576, FR_SZ = 32;
 constexpr size_t LINE_SZ = 288;  // three Fp2 coefficients
 constexpr int LINES_PER_POINT = 68;
@@ -103,5 +114,7 @@ void launch_unmask(uint8_t* out, const uint8_t* second, const uint8_t* alpha, co
 void launch_gt_compress(uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
 // flags[i] = (in[i] == 1)
 void launch_fp12_is_one(uint8_t* flags, const uint8_t* in, int64_t n, cudaStream_t s);
+// sustained 32-bit IMAD instructions per second (calibration kernel, synchronising)
+double measure_imad_rate(cudaStream_t s);
 
 }  // namespace wbte

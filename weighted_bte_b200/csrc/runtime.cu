@@ -17,7 +17,36 @@ using namespace wbte;
 
 namespace wbte {
 std::atomic<uint64_t> g_launches{0};
+
+namespace {
+struct ProfRec {
+    const char* tag;
+    cudaEvent_t a, b;
+};
+std::mutex g_prof_mu;
+std::vector<ProfRec> g_prof;
+std::atomic<bool> g_prof_on{false};
+}  // namespace
+
+void prof_begin(const char* tag, cudaStream_t s, void** token) {
+    *token = nullptr;
+    if (!g_prof_on.load(std::memory_order_relaxed)) return;
+    ProfRec* r = new ProfRec{tag, nullptr, nullptr};
+    cudaEventCreate(&r->a);
+    cudaEventCreate(&r->b);
+    cudaEventRecord(r->a, s);
+    *token = r;
 }
+
+void prof_end(void* token, cudaStream_t s) {
+    if (!token) return;
+    ProfRec* r = static_cast<ProfRec*>(token);
+    cudaEventRecord(r->b, s);
+    std::lock_guard<std::mutex> lock(g_prof_mu);
+    g_prof.push_back(*r);
+    delete r;
+}
+}  // namespace wbte
 
 struct wbte_ctx {
     int device = 0;
@@ -305,6 +334,60 @@ const char* wbte_ctx_last_error(const wbte_ctx* ctx) { return ctx ? ctx->err.c_s
 uint64_t wbte_ctx_launch_count(const wbte_ctx* ctx) {
     (void)ctx;
     return g_launches.load();
+}
+
+int32_t wbte_measure_imad_rate(wbte_ctx* ctx, double* imad_per_s) {
+    if (!ctx || !imad_per_s) return WBTE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    *imad_per_s = measure_imad_rate(ctx->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        ctx->err = cudaGetErrorString(e);
+        return WBTE_ERR_CUDA;
+    }
+    return WBTE_OK;
+}
+
+int32_t wbte_profile_enable(int32_t on) {
+    std::lock_guard<std::mutex> lock(g_prof_mu);
+    for (auto& r : g_prof) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_prof.clear();
+    g_prof_on.store(on != 0);
+    return WBTE_OK;
+}
+
+int32_t wbte_profile_read(char* names, int32_t name_stride, double* ms, int64_t* counts, int32_t max_entries,
+                          int32_t* n_out) {
+    if (!n_out || name_stride < 2) return WBTE_ERR_INVALID_ARG;
+    if (cudaDeviceSynchronize() != cudaSuccess) return WBTE_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_prof_mu);
+    std::map<std::string, std::pair<double, int64_t>> agg;
+    for (auto& r : g_prof) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, r.a, r.b) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        auto& e = agg[r.tag];
+        e.first += t;
+        e.second += 1;
+    }
+    int32_t i = 0;
+    for (auto& kv : agg) {
+        if (i >= max_entries) break;
+        if (names) {
+            std::strncpy(names + (size_t)i * name_stride, kv.first.c_str(), name_stride - 1);
+            names[(size_t)i * name_stride + name_stride - 1] = 0;
+        }
+        if (ms) ms[i] = kv.second.first;
+        if (counts) counts[i] = kv.second.second;
+        i++;
+    }
+    *n_out = i;
+    return WBTE_OK;
 }
 
 // ------------------------------------------------------------------ MSM

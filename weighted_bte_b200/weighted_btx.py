@@ -1,0 +1,893 @@
+"""Weighted BTX batched threshold encryption (Construction 1) on B200.
+
+Mirrors the public API of the reference crate `weighted_btx`
+(weighted_btx/src/lib.rs:21-31): `keygen[_with_rng]`, `encrypt[_with_rng]`,
+`validate_batch`, `partial_decrypt`, `verify_decryption_share`,
+`accept_decryption_shares`, `prepare_decryption`, `precompute_batch`,
+`open_batch`, `decrypt`, with the same argument meaning, the same checks and
+the same error variants (weighted_bte_b200.errors).
+
+Every group operation runs in libwbte (sm_100a kernels behind include/wbte.h);
+this module holds the protocol logic: argument checks, SHA-256 transcripts
+(host hashlib, as the reference uses sha2) and the data layout.  The public
+decryption key is resident in HBM.  Group elements are `bytes` in blst's
+memory layout (G1 96 B, G2 192 B, GT 576 B); scalars are Python ints.
+"""
+from __future__ import annotations
+
+import hashlib
+import struct
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib, ops
+from . import errors as E
+from .rng import OsRng, random_scalar, sample_nonzero
+
+R = ops.R
+G1B, G2B, GTB = _lib.G1_BYTES, _lib.G2_BYTES, _lib.GT_BYTES
+SETUP_ID_DOMAIN = b"WEIGHTED-BTX-SETUP-ID-v1"
+TRANSCRIPT_DOMAIN = b"WEIGHTED-BTX-SCHNORR-BLS12381-v1"
+BATCH_DIGEST_DOMAIN = b"WEIGHTED-BTX-ORDERED-BATCH-v1"
+DECRYPTION_CONTEXT_DOMAIN = b"WEIGHTED-BTX-DECRYPTION-CONTEXT-v1"
+G1_IDENTITY = bytes(G1B)
+ROOT_OF_UNITY = pow(7, (R - 1) >> 32, R)
+TWO_ADICITY = 32
+
+# ------------------------------------------------------------ device memory
+_torch = None
+
+
+def _t():
+    global _torch
+    if _torch is None:
+        import torch
+
+        _torch = torch
+    return _torch
+
+
+def _device(device: int = 0):
+    return _t().device("cuda", device)
+
+
+def to_device(data: bytes, device: int = 0):
+    torch = _t()
+    if len(data) == 0:
+        return torch.empty(16, dtype=torch.uint8, device=_device(device))
+    return torch.frombuffer(bytearray(data), dtype=torch.uint8).to(_device(device))
+
+
+def empty_device(nbytes: int, device: int = 0):
+    return _t().empty(max(16, nbytes), dtype=torch_uint8(), device=_device(device))
+
+
+def torch_uint8():
+    return _t().uint8
+
+
+def to_host(tensor, nbytes: Optional[int] = None) -> bytes:
+    data = tensor.detach().cpu().numpy().tobytes()
+    return data if nbytes is None else data[:nbytes]
+
+
+def _ctx():
+    ctx = ops.ctx()
+    torch = _t()
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    return ctx
+
+
+# ----------------------------------------------------------- field helpers
+def fr_bytes(s: int) -> bytes:
+    return (s % R).to_bytes(32, "little")
+
+
+def radix2_generator(size: int) -> int:
+    """Generator of the size-`size` subgroup (btx/src/fft.rs:165-178)."""
+    if size <= 0 or size & (size - 1):
+        raise E.InvalidBatchSize(size)
+    lg = size.bit_length() - 1
+    if lg > TWO_ADICITY:
+        raise E.InvalidBatchSize(size)
+    g = ROOT_OF_UNITY
+    for _ in range(lg, TWO_ADICITY):
+        g = g * g % R
+    return g
+
+
+def scalar_fft(values: List[int], size: int) -> List[int]:
+    """Radix-2 Fr transform (host; used for the Shamir evaluations of keygen)."""
+    g = radix2_generator(size)
+    a = list(values) + [0] * (size - len(values))
+    bits = size.bit_length() - 1
+    for i in range(size):
+        j = int(format(i, f"0{bits}b")[::-1], 2) if bits else 0
+        if i < j:
+            a[i], a[j] = a[j], a[i]
+    m = 2
+    while m <= size:
+        w_m = pow(g, size // m, R)
+        for k in range(0, size, m):
+            w = 1
+            for j in range(m // 2):
+                t = w * a[k + j + m // 2] % R
+                u = a[k + j]
+                a[k + j] = (u + t) % R
+                a[k + j + m // 2] = (u - t) % R
+                w = w * w_m % R
+        m *= 2
+    return a
+
+
+_GT_GEN = None
+_G1_GEN = None
+
+
+def g1_generator() -> bytes:
+    global _G1_GEN
+    if _G1_GEN is None:
+        _G1_GEN = ops.g1_mul_generator([1])
+    return _G1_GEN
+
+
+def gt_generator() -> bytes:
+    """e(G1, G2) -- blstrs `Gt::generator()`."""
+    global _GT_GEN
+    if _GT_GEN is None:
+        g2 = ops.g2_mul_generator([1])
+        _GT_GEN = ops.pairing(g1_generator(), g2)
+    return _GT_GEN
+
+
+GT_IDENTITY = None
+
+
+def gt_identity() -> bytes:
+    one = bytearray(GTB)
+    # Montgomery one = R mod p in the first coefficient
+    p = 0x1A0111EA397FE69A4B1BA7B6434BACD764774B84F38512BF6730D2A0F6B0F6241EABFFFEB153FFFFB9FEFFFFFFFFAAAB
+    one[:48] = ((1 << 384) % p).to_bytes(48, "little")
+    return bytes(one)
+
+
+def message_from_bytes(data: bytes) -> bytes:
+    """Map a byte string to GT: Gt::generator()^(LE(data) mod r)."""
+    return ops.gt_pow(gt_generator(), [int.from_bytes(data, "little") % R], fixed_base=True)
+
+
+def messages_from_bytes(datas: Sequence[bytes]) -> List[bytes]:
+    if not datas:
+        return []
+    sc = [int.from_bytes(d, "little") % R for d in datas]
+    return ops.split(ops.gt_pow(gt_generator(), sc, fixed_base=True), GTB)
+
+
+def append_gt_many(values: bytes, n: int) -> List[bytes]:
+    enc = ops.gt_compress(values, n)
+    out = []
+    for i in range(n):
+        rec = enc[289 * i : 289 * (i + 1)]
+        out.append(rec[:1] if rec[0] == 0 else rec)
+    return out
+
+
+# ------------------------------------------------------------------- keys
+@dataclass
+class KeygenConfig:
+    max_batch_size: int
+    party_weights: List[int]
+    threshold_weight: int
+
+
+@dataclass
+class EncryptionKey:
+    _max_batch_size: int
+    _element: bytes
+    _setup_id: bytes
+
+    def max_batch_size(self) -> int:
+        return self._max_batch_size
+
+    def element(self) -> bytes:
+        return self._element
+
+    def setup_id(self) -> bytes:
+        return self._setup_id
+
+
+class PublicDecryptionKey:
+    """Public weighted-BTX decryption material, resident in HBM.
+
+    Layout as in weighted_btx/src/setup.rs:28-51: exponent-major blocks of
+    verification keys [q_j^i]_2 (index (i-1) N + j), negative material
+    [Z(w) q_owner(w)^-i]_2 and positive material [Z(w) q_owner(w)^i]_2
+    (index (i-1) W + w).
+    """
+
+    def __init__(self, setup_id, max_batch_size, threshold_weight, total_weight, domain_size, party_weights,
+                 party_offsets, evaluation_domain, verification_keys, negative_material, positive_material):
+        self._setup_id = setup_id
+        self._max_batch_size = max_batch_size
+        self._threshold_weight = threshold_weight
+        self._total_weight = total_weight
+        self._domain_size = domain_size
+        self._party_weights = list(party_weights)
+        self.party_offsets = np.asarray(party_offsets, dtype=np.int64)
+        self._evaluation_domain = list(evaluation_domain)
+        self.domain_dev = to_device(b"".join(fr_bytes(x) for x in evaluation_domain))
+        self.verification_keys = verification_keys
+        self.negative_material = negative_material
+        self.positive_material = positive_material
+
+    def setup_id(self) -> bytes:
+        return self._setup_id
+
+    def max_batch_size(self) -> int:
+        return self._max_batch_size
+
+    def party_count(self) -> int:
+        return len(self._party_weights)
+
+    def total_weight(self) -> int:
+        return self._total_weight
+
+    def threshold_weight(self) -> int:
+        return self._threshold_weight
+
+    def required_weight(self) -> int:
+        return self._threshold_weight + 1
+
+    def party_weights(self) -> List[int]:
+        return list(self._party_weights)
+
+    def party_weight(self, party_index: int) -> int:
+        if not 0 <= party_index < self.party_count():
+            raise E.InvalidPartyIndex(party_index)
+        return self._party_weights[party_index]
+
+    def domain_points(self) -> List[int]:
+        return list(self._evaluation_domain)
+
+    def domain_size(self) -> int:
+        return self._domain_size
+
+    def party_range(self, party_index: int) -> range:
+        if not 0 <= party_index < self.party_count():
+            raise E.InvalidPartyIndex(party_index)
+        return range(int(self.party_offsets[party_index]), int(self.party_offsets[party_index + 1]))
+
+    def _validate_power(self, power: int, max_power: int):
+        if power == 0 or power > max_power:
+            raise E.InvalidPower(power, max_power)
+
+    def verification_key(self, party_index: int, power: int) -> bytes:
+        if not 0 <= party_index < self.party_count():
+            raise E.InvalidPartyIndex(party_index)
+        self._validate_power(power, self._max_batch_size)
+        i = (power - 1) * self.party_count() + party_index
+        return to_host(self.verification_keys[G2B * i : G2B * (i + 1)])
+
+    def verification_power(self, power: int) -> List[bytes]:
+        self._validate_power(power, self._max_batch_size)
+        n = self.party_count()
+        return ops.split(to_host(self.verification_keys[G2B * (power - 1) * n : G2B * power * n]), G2B)
+
+    def negative_power(self, power: int) -> List[bytes]:
+        self._validate_power(power, self._max_batch_size)
+        W = self._total_weight
+        return ops.split(to_host(self.negative_material[G2B * (power - 1) * W : G2B * power * W]), G2B)
+
+    def positive_power(self, power: int) -> List[bytes]:
+        self._validate_power(power, max(0, self._max_batch_size - 1))
+        W = self._total_weight
+        return ops.split(to_host(self.positive_material[G2B * (power - 1) * W : G2B * power * W]), G2B)
+
+    def abi_key(self) -> _lib.WbtxKey:
+        k = _lib.WbtxKey()
+        k.domain_points = self.domain_dev.data_ptr()
+        k.verification_keys = self.verification_keys.data_ptr()
+        k.negative_material = self.negative_material.data_ptr()
+        k.positive_material = self.positive_material.data_ptr()
+        self._offsets_keep = np.ascontiguousarray(self.party_offsets, dtype=np.int64)
+        k.party_offsets = self._offsets_keep.ctypes.data
+        k.party_count = self.party_count()
+        k.total_weight = self._total_weight
+        k.max_batch_size = self._max_batch_size
+        return k
+
+
+@dataclass
+class PartySecretKey:
+    party_index: int
+    _setup_id: bytes
+    _max_batch_size: int
+    _q: int
+
+    def setup_id(self) -> bytes:
+        return self._setup_id
+
+    def max_batch_size(self) -> int:
+        return self._max_batch_size
+
+    def secret_scalar(self) -> int:
+        return self._q
+
+
+@dataclass
+class KeyMaterial:
+    encryption_key: EncryptionKey
+    decryption_key: PublicDecryptionKey
+    party_keys: List[PartySecretKey]
+
+
+def _validate_config(config: KeygenConfig):
+    if config.max_batch_size == 0:
+        raise E.BatchIsEmpty()
+    if not config.party_weights:
+        raise E.EmptyCommittee()
+    for j, w in enumerate(config.party_weights):
+        if w == 0:
+            raise E.InvalidPartyWeight(j, w)
+    total = sum(config.party_weights)
+    if total >= 1 << 64:
+        raise E.TotalWeightOverflow()
+    if config.threshold_weight >= total:
+        raise E.InvalidCommittee(len(config.party_weights), total, config.threshold_weight)
+    domain = 1 << (total - 1).bit_length() if total > 1 else 1
+    if domain.bit_length() - 1 > TWO_ADICITY:
+        raise E.InvalidEvaluationDomain(total)
+    if config.max_batch_size * total * G2B >= 1 << 63:
+        raise E.ParameterSizeOverflow()
+    return total, domain
+
+
+def setup_identifier(ek_element: bytes, max_batch_size: int, threshold: int, weights: Sequence[int],
+                     first_vk_compressed: bytes, first_neg_compressed: bytes) -> bytes:
+    """weighted_btx/src/setup.rs:486-513."""
+    h = hashlib.sha256()
+    h.update(SETUP_ID_DOMAIN)
+    h.update(struct.pack("<Q", max_batch_size))
+    h.update(struct.pack("<Q", threshold))
+    h.update(struct.pack("<Q", len(weights)))
+    for w in weights:
+        h.update(struct.pack("<Q", w))
+    h.update(append_gt_many(ek_element, 1)[0])
+    h.update(first_vk_compressed)
+    h.update(first_neg_compressed)
+    return h.digest()
+
+
+def keygen_with_rng(config: KeygenConfig, rng) -> KeyMaterial:
+    """Trusted-dealer setup (weighted_btx/src/setup.rs:98-233).
+
+    Scalar draws follow the reference: t+1 polynomial coefficients, then one
+    nonzero secret per party.  The (2L - 1) W + N L fixed-base G2
+    multiplications run on the GPU.
+    """
+    total, domain = _validate_config(config)
+    N, L, W = len(config.party_weights), config.max_batch_size, total
+    coeffs = [random_scalar(rng) for _ in range(config.threshold_weight + 1)]
+    z = coeffs[0]
+    z_evals = scalar_fft(coeffs, domain)[:W]
+    g = radix2_generator(domain)
+    evaluation_domain = [pow(g, i, R) for i in range(W)] if domain > 1 else [1]
+    offsets = np.zeros(N + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum(config.party_weights)
+    owner = np.repeat(np.arange(N, dtype=np.int32), config.party_weights)
+    qs = [sample_nonzero(rng) for _ in range(N)]
+    qpos = bytearray(32 * L * N)
+    qneg = bytearray(32 * L * N)
+    for j, q in enumerate(qs):
+        qi = pow(q, R - 2, R)
+        p, n = q, qi
+        for i in range(L):
+            idx = 32 * (i * N + j)
+            qpos[idx : idx + 32] = fr_bytes(p)
+            qneg[idx : idx + 32] = fr_bytes(n)
+            p = p * q % R
+            n = n * qi % R
+    vk = empty_device(G2B * L * N)
+    neg = empty_device(G2B * L * W)
+    pos = empty_device(G2B * max(1, (L - 1) * W))
+    ctx = _ctx()
+    ctx.call("wbte_wbtx_keygen_material", b"".join(fr_bytes(x) for x in z_evals), _lib.i32_array(owner),
+             bytes(qpos), bytes(qneg), W, N, L, vk, neg, pos)
+    element = ops.gt_pow(gt_generator(), [z], fixed_base=True)
+    vk_c = ops.g2_compress(vk[: G2B * N], N)
+    neg_c = ops.g2_compress(neg[: G2B * W], W)
+    setup_id = setup_identifier(element, L, config.threshold_weight, config.party_weights, vk_c, neg_c)
+    dk = PublicDecryptionKey(setup_id, L, config.threshold_weight, W, domain, config.party_weights, offsets,
+                             evaluation_domain, vk, neg, pos)
+    ek = EncryptionKey(L, element, setup_id)
+    parties = [PartySecretKey(j, setup_id, L, q) for j, q in enumerate(qs)]
+    return KeyMaterial(ek, dk, parties)
+
+
+def keygen(max_batch_size: int, party_weights: Sequence[int], threshold_weight: int) -> KeyMaterial:
+    return keygen_with_rng(KeygenConfig(max_batch_size, list(party_weights), threshold_weight), OsRng())
+
+
+# ------------------------------------------------------------- encryption
+@dataclass
+class SchnorrProof:
+    commitment: bytes  # G1 affine
+    response: int
+
+
+@dataclass
+class Ciphertext:
+    first: bytes  # G1 affine
+    second: bytes  # GT
+    proof: SchnorrProof
+
+    def verify(self, encryption_key: EncryptionKey) -> bool:
+        return bool(verify_ciphertexts([self], encryption_key.setup_id())[0])
+
+
+def _challenges(setup_id: bytes, first_c: List[bytes], second_enc: List[bytes], comm_c: List[bytes]) -> List[int]:
+    """Fiat-Shamir challenge with rejection sampling (weighted_btx/src/proof.rs:156-185)."""
+    gen_c = ops.g1_compress(g1_generator(), 1)
+    out = []
+    for a, b, c in zip(first_c, second_enc, comm_c):
+        prefix = TRANSCRIPT_DOMAIN + setup_id + gen_c + a + b + c
+        counter = 0
+        while True:
+            d = hashlib.sha256(prefix + struct.pack("<I", counter)).digest()
+            v = int.from_bytes(d, "little")
+            if v < R:
+                out.append(v)
+                break
+            counter += 1
+    return out
+
+
+def encrypt_many(encryption_key: EncryptionKey, messages: Sequence[bytes], rng) -> List[Ciphertext]:
+    """Batched `encrypt_with_rng` (weighted_btx/src/encryption.rs:28-49);
+    draws (randomness, nonce) per message in order, as sequential calls would."""
+    n = len(messages)
+    if n == 0:
+        return []
+    rs, ks = [], []
+    for _ in range(n):
+        rs.append(random_scalar(rng))
+        ks.append(random_scalar(rng))
+    first = ops.g1_mul_generator(rs)
+    comm = ops.g1_mul_generator(ks)
+    mask = ops.gt_pow(encryption_key.element(), rs, fixed_base=True)
+    second = ops.fp12_mul(b"".join(messages), mask)
+    first_c = ops.split(ops.g1_compress(first, n), 48)
+    comm_c = ops.split(ops.g1_compress(comm, n), 48)
+    second_enc = append_gt_many(second, n)
+    cs = _challenges(encryption_key.setup_id(), first_c, second_enc, comm_c)
+    out = []
+    for i in range(n):
+        resp = (ks[i] + cs[i] * rs[i]) % R
+        out.append(Ciphertext(first[G1B * i : G1B * (i + 1)], second[GTB * i : GTB * (i + 1)],
+                              SchnorrProof(comm[G1B * i : G1B * (i + 1)], resp)))
+    return out
+
+
+def encrypt_with_rng(encryption_key: EncryptionKey, message: bytes, rng) -> Ciphertext:
+    return encrypt_many(encryption_key, [message], rng)[0]
+
+
+def encrypt(encryption_key: EncryptionKey, message: bytes) -> Ciphertext:
+    return encrypt_with_rng(encryption_key, message, OsRng())
+
+
+class CiphertextBatch:
+    """An ordered ciphertext batch resident in HBM.
+
+    The group elements live in device arrays (G1 first components, GT second
+    components, G1 proof commitments); the proof responses stay on the host.
+    The batch is immutable, so its canonical encodings and digest are
+    computed once and cached.
+    """
+
+    def __init__(self, first, second, commitment, responses: Sequence[int]):
+        self.first, self.second, self.commitment = first, second, commitment
+        self.responses = [int(r) for r in responses]
+        self._enc = None
+        self._digest = None
+
+    @classmethod
+    def upload(cls, cts: Sequence[Ciphertext]) -> "CiphertextBatch":
+        return cls(to_device(b"".join(c.first for c in cts)), to_device(b"".join(c.second for c in cts)),
+                   to_device(b"".join(c.proof.commitment for c in cts)), [c.proof.response for c in cts])
+
+    def __len__(self) -> int:
+        return len(self.responses)
+
+    def to_ciphertexts(self) -> List[Ciphertext]:
+        n = len(self)
+        f, s, c = to_host(self.first, G1B * n), to_host(self.second, GTB * n), to_host(self.commitment, G1B * n)
+        return [Ciphertext(f[G1B * i : G1B * (i + 1)], s[GTB * i : GTB * (i + 1)],
+                           SchnorrProof(c[G1B * i : G1B * (i + 1)], self.responses[i])) for i in range(n)]
+
+    def encodings(self):
+        if self._enc is None:
+            n = len(self)
+            first_c = ops.split(ops.g1_compress(self.first, n), 48)
+            comm_c = ops.split(ops.g1_compress(self.commitment, n), 48)
+            self._enc = (self.first, self.commitment, first_c, comm_c, append_gt_many(self.second, n))
+        return self._enc
+
+    def digest(self) -> bytes:
+        if self._digest is None:
+            _, _, first_c, comm_c, second_enc = self.encodings()
+            h = hashlib.sha256()
+            h.update(BATCH_DIGEST_DOMAIN)
+            h.update(struct.pack("<Q", len(self)))
+            for i, r in enumerate(self.responses):
+                h.update(_canonical(first_c[i], second_enc[i], comm_c[i], r))
+            self._digest = h.digest()
+        return self._digest
+
+
+def _encodings(cts):
+    if isinstance(cts, CiphertextBatch):
+        return cts.encodings()
+    n = len(cts)
+    first = b"".join(c.first for c in cts)
+    comm = b"".join(c.proof.commitment for c in cts)
+    second = b"".join(c.second for c in cts)
+    first_c = ops.split(ops.g1_compress(first, n), 48)
+    comm_c = ops.split(ops.g1_compress(comm, n), 48)
+    second_enc = append_gt_many(second, n)
+    return first, comm, first_c, comm_c, second_enc
+
+
+def _responses(cts) -> List[int]:
+    if isinstance(cts, CiphertextBatch):
+        return cts.responses
+    return [c.proof.response for c in cts]
+
+
+def verify_ciphertexts(cts: Sequence[Ciphertext], setup_id: bytes, encodings=None) -> np.ndarray:
+    """Batched `Ciphertext::verify_for_setup` (weighted_btx/src/encryption.rs:57-59)."""
+    if len(cts) == 0:
+        return np.zeros(0, dtype=bool)
+    first, comm, first_c, comm_c, second_enc = encodings or _encodings(cts)
+    cs = _challenges(setup_id, first_c, second_enc, comm_c)
+    out = np.zeros(len(cts), dtype=np.uint8)
+    ops.ctx().call("wbte_schnorr_verify", out, first, comm, ops.scalars_bytes(_responses(cts)),
+                   ops.scalars_bytes(cs), len(cts))
+    return out.astype(bool)
+
+
+def _canonical(first_c: bytes, second_enc: bytes, comm_c: bytes, response: int) -> bytes:
+    return first_c + second_enc + comm_c + fr_bytes(response)
+
+
+def batch_digest(cts, encodings=None) -> bytes:
+    """weighted_btx/src/decryption.rs:740-748."""
+    if isinstance(cts, CiphertextBatch):
+        return cts.digest()
+    _, _, first_c, comm_c, second_enc = encodings or _encodings(cts)
+    h = hashlib.sha256()
+    h.update(BATCH_DIGEST_DOMAIN)
+    h.update(struct.pack("<Q", len(cts)))
+    for i, ct in enumerate(cts):
+        h.update(_canonical(first_c[i], second_enc[i], comm_c[i], ct.proof.response))
+    return h.digest()
+
+
+def decryption_context_id(setup_id: bytes, batch_size: int, party_indices: Sequence[int]) -> bytes:
+    """weighted_btx/src/decryption.rs:750-764."""
+    h = hashlib.sha256()
+    h.update(DECRYPTION_CONTEXT_DOMAIN)
+    h.update(setup_id)
+    h.update(struct.pack("<Q", batch_size))
+    h.update(struct.pack("<Q", len(party_indices)))
+    for j in party_indices:
+        h.update(struct.pack("<Q", j))
+    return h.digest()
+
+
+# -------------------------------------------------------------- decryption
+@dataclass
+class ValidatedBatch:
+    _setup_id: bytes
+    _batch_size: int
+    _digest: bytes
+    valid: np.ndarray
+    first_affine: bytes
+    first_dev: object = None
+    valid_dev: object = None
+
+    def batch_size(self) -> int:
+        return self._batch_size
+
+    def setup_id(self) -> bytes:
+        return self._setup_id
+
+    def digest(self) -> bytes:
+        return self._digest
+
+    def valid_mask(self) -> List[bool]:
+        return [bool(v) for v in self.valid]
+
+    def valid_count(self) -> int:
+        return int(self.valid.sum())
+
+
+@dataclass
+class DecryptionShare:
+    party_index: int
+    sigma: bytes  # G1 affine
+    batch_digest: bytes
+    setup_id: bytes
+
+
+@dataclass
+class AcceptedDecryptionShares:
+    setup_id: bytes
+    batch_size: int
+    digest: bytes
+    _accepted_weight: int
+    _shares: List[DecryptionShare]
+    _rejected_parties: List[int]
+
+    def accepted_weight(self) -> int:
+        return self._accepted_weight
+
+    def party_count(self) -> int:
+        return len(self._shares)
+
+    def party_indices(self) -> List[int]:
+        return [s.party_index for s in self._shares]
+
+    def rejected_parties(self) -> List[int]:
+        return list(self._rejected_parties)
+
+    def shares(self) -> List[DecryptionShare]:
+        return list(self._shares)
+
+
+@dataclass
+class DecryptionPrecomputation:
+    setup_id: bytes
+    context_id: bytes
+    _batch_size: int
+    _accepted_weight: int
+    party_indices: List[int]
+    _transform_size: int
+    kernel_lines: object  # device, m * 68 * 288 bytes
+    opening_keys: object  # device, B * T G2
+    transformed_kernel: object  # device, m G2
+
+    def batch_size(self) -> int:
+        return self._batch_size
+
+    def accepted_weight(self) -> int:
+        return self._accepted_weight
+
+    def party_count(self) -> int:
+        return len(self.party_indices)
+
+    def transform_size(self) -> int:
+        return self._transform_size
+
+
+@dataclass
+class BatchPrecomputation:
+    context_id: bytes
+    batch_size: int
+    digest: bytes
+    beta: object  # device, B GT
+
+
+def _validate_batch_size(dk: PublicDecryptionKey, batch_size: int):
+    if batch_size == 0:
+        raise E.BatchIsEmpty()
+    if batch_size > dk.max_batch_size():
+        raise E.BatchTooLarge(batch_size, dk.max_batch_size())
+
+
+def validate_batch(decryption_key: PublicDecryptionKey, ciphertexts: Sequence[Ciphertext]) -> ValidatedBatch:
+    """weighted_btx/src/decryption.rs:85-140: verify every proof, keep slot positions."""
+    _validate_batch_size(decryption_key, len(ciphertexts))
+    enc = _encodings(ciphertexts)
+    valid = verify_ciphertexts(ciphertexts, decryption_key.setup_id(), enc)
+    valid_dev = to_device(valid.astype(np.uint8).tobytes())
+    if isinstance(ciphertexts, CiphertextBatch):
+        n = len(ciphertexts)
+        first_dev = (ciphertexts.first[: G1B * n].view(n, G1B) * valid_dev[:n].view(n, 1)).reshape(-1)
+        first = None
+    else:
+        first = b"".join(ct.first if v else G1_IDENTITY for ct, v in zip(ciphertexts, valid))
+        first_dev = to_device(first)
+    return ValidatedBatch(decryption_key.setup_id(), len(ciphertexts), batch_digest(ciphertexts, enc),
+                          valid, first, first_dev, valid_dev)
+
+
+def partial_decrypt_many(party_keys: Sequence[PartySecretKey], batch: ValidatedBatch) -> List[DecryptionShare]:
+    """`partial_decrypt` for several parties in one launch sequence
+    (weighted_btx/src/decryption.rs:205-233)."""
+    for pk in party_keys:
+        if batch.setup_id() != pk.setup_id():
+            raise E.MismatchedSetup()
+        if batch.batch_size() > pk.max_batch_size():
+            raise E.BatchTooLarge(batch.batch_size(), pk.max_batch_size())
+    T = len(party_keys)
+    if T == 0:
+        return []
+    sig = bytearray(G1B * T)
+    _ctx().call("wbte_wbtx_partial_decrypt", sig, batch.first_dev, batch.batch_size(),
+                b"".join(fr_bytes(pk.secret_scalar()) for pk in party_keys), T)
+    return [DecryptionShare(pk.party_index, bytes(sig[G1B * j : G1B * (j + 1)]), batch.digest(), pk.setup_id())
+            for j, pk in enumerate(party_keys)]
+
+
+def partial_decrypt(party_key: PartySecretKey, batch: ValidatedBatch) -> DecryptionShare:
+    return partial_decrypt_many([party_key], batch)[0]
+
+
+def _verify_shares(dk: PublicDecryptionKey, batch: ValidatedBatch, shares: Sequence[DecryptionShare],
+                   challenges: Sequence[int]) -> bool:
+    ok = np.zeros(1, dtype=np.int32)
+    T = len(shares)
+    _ctx().call("wbte_wbtx_verify_shares", ok, dk.abi_key(), batch.first_dev, batch.valid_dev, batch.batch_size(),
+                b"".join(s.sigma for s in shares), _lib.i64_array([s.party_index for s in shares]),
+                b"".join(fr_bytes(c) for c in challenges), T)
+    return bool(ok[0])
+
+
+def verify_decryption_share(decryption_key: PublicDecryptionKey, batch: ValidatedBatch,
+                            share: DecryptionShare) -> bool:
+    """weighted_btx/src/decryption.rs:236-272."""
+    _validate_batch_size(decryption_key, batch.batch_size())
+    if batch.setup_id() != decryption_key.setup_id():
+        raise E.MismatchedSetup()
+    if share.batch_digest != batch.digest() or share.setup_id != decryption_key.setup_id():
+        return False
+    if share.party_index >= decryption_key.party_count():
+        raise E.InvalidPartyIndex(share.party_index)
+    return _verify_shares(decryption_key, batch, [share], [1])
+
+
+def accept_decryption_shares(decryption_key: PublicDecryptionKey, batch: ValidatedBatch,
+                             shares: Sequence[DecryptionShare], rng=None) -> AcceptedDecryptionShares:
+    """weighted_btx/src/decryption.rs:276-353 (batched check, per-share fallback, weight check)."""
+    _validate_batch_size(decryption_key, batch.batch_size())
+    if batch.setup_id() != decryption_key.setup_id():
+        raise E.MismatchedSetup()
+    if len(shares) > decryption_key.party_count():
+        raise E.TooManyShares(len(shares), decryption_key.party_count())
+    seen = [False] * decryption_key.party_count()
+    candidates, rejected = [], []
+    for s in shares:
+        if s.party_index >= decryption_key.party_count():
+            raise E.InvalidPartyIndex(s.party_index)
+        if seen[s.party_index]:
+            raise E.DuplicatePartyIndex(s.party_index)
+        seen[s.party_index] = True
+        if s.batch_digest == batch.digest() and s.setup_id == decryption_key.setup_id():
+            candidates.append(s)
+        else:
+            rejected.append(s.party_index)
+    rng = rng or OsRng()
+    if candidates:
+        challenges = [sample_nonzero(rng) for _ in candidates]
+        aggregate_ok = _verify_shares(decryption_key, batch, candidates, challenges)
+    else:
+        aggregate_ok = True
+    if aggregate_ok:
+        accepted = candidates
+    else:
+        accepted = []
+        for s in candidates:
+            if verify_decryption_share(decryption_key, batch, s):
+                accepted.append(s)
+            else:
+                rejected.append(s.party_index)
+    accepted.sort(key=lambda s: s.party_index)
+    rejected.sort()
+    weight = sum(decryption_key.party_weight(s.party_index) for s in accepted)
+    if weight <= decryption_key.threshold_weight():
+        raise E.InsufficientWeight(weight, decryption_key.required_weight(), rejected)
+    return AcceptedDecryptionShares(decryption_key.setup_id(), batch.batch_size(), batch.digest(), weight, accepted,
+                                    rejected)
+
+
+def transform_size_for(batch_size: int) -> int:
+    return 1 << (2 * batch_size - 1).bit_length()
+
+
+def prepare_decryption(decryption_key: PublicDecryptionKey,
+                       accepted: AcceptedDecryptionShares) -> DecryptionPrecomputation:
+    """weighted_btx/src/decryption.rs:427-551 (committee-dependent G2 work, cacheable)."""
+    _validate_batch_size(decryption_key, accepted.batch_size)
+    if accepted.setup_id != decryption_key.setup_id():
+        raise E.MismatchedSetup()
+    if accepted.accepted_weight() <= decryption_key.threshold_weight():
+        raise E.InsufficientWeight(accepted.accepted_weight(), decryption_key.required_weight(), [])
+    parties = accepted.party_indices()
+    B = accepted.batch_size
+    m = transform_size_for(B)
+    lines = empty_device(_lib.LINE_BYTES * _lib.MILLER_LINES * m)
+    opening = empty_device(G2B * B * len(parties))
+    kernel = empty_device(G2B * m)
+    try:
+        _ctx().call("wbte_wbtx_prepare", decryption_key.abi_key(), _lib.i64_array(parties), len(parties), B, lines,
+                    opening, kernel)
+    except _lib.WbteError as exc:
+        if exc.status == -7:
+            raise E.InvalidInterpolationSet() from exc
+        raise
+    ctx_id = decryption_context_id(decryption_key.setup_id(), B, parties)
+    return DecryptionPrecomputation(decryption_key.setup_id(), ctx_id, B, accepted.accepted_weight(), parties, m,
+                                    lines, opening, kernel)
+
+
+def _ensure_precomputation_batch(pre: DecryptionPrecomputation, batch: ValidatedBatch):
+    if pre.batch_size() != batch.batch_size():
+        raise E.MismatchedBatchSize(pre.batch_size(), batch.batch_size())
+    if pre.setup_id != batch.setup_id():
+        raise E.MismatchedSetup()
+
+
+def precompute_batch(precomputation: DecryptionPrecomputation, batch: ValidatedBatch) -> BatchPrecomputation:
+    """weighted_btx/src/decryption.rs:555-603 (middle product via G1 NTT, prepared
+    Miller loops, easy part, truncated cyclotomic inverse transform, hard part)."""
+    _ensure_precomputation_batch(precomputation, batch)
+    B = batch.batch_size()
+    beta = empty_device(GTB * B)
+    _ctx().call("wbte_wbtx_precompute", beta, precomputation.kernel_lines, batch.first_dev, batch.valid_dev, B)
+    return BatchPrecomputation(precomputation.context_id, B, batch.digest(), beta)
+
+
+def open_batch(precomputation: DecryptionPrecomputation, accepted: AcceptedDecryptionShares, batch: ValidatedBatch,
+               ciphertexts, cross_terms: BatchPrecomputation, device_output: bool = False):
+    """weighted_btx/src/decryption.rs:607-695.
+
+    Returns one `Optional[bytes]` per slot (None for invalid slots), or with
+    device_output=True a device array of B GT values (identity at invalid
+    slots) that stays in HBM."""
+    _ensure_precomputation_batch(precomputation, batch)
+    if accepted.batch_size != batch.batch_size():
+        raise E.MismatchedBatchSize(batch.batch_size(), accepted.batch_size)
+    if accepted.digest != batch.digest():
+        raise E.MismatchedBatchDigest()
+    if len(ciphertexts) != batch.batch_size():
+        raise E.MismatchedBatchSize(batch.batch_size(), len(ciphertexts))
+    if batch_digest(ciphertexts) != batch.digest():
+        raise E.MismatchedBatchDigest()
+    if cross_terms.batch_size != batch.batch_size() or cross_terms.digest != batch.digest():
+        raise E.MismatchedBatchDigest()
+    if cross_terms.context_id != precomputation.context_id:
+        raise E.MismatchedCommittee()
+    if accepted.setup_id != precomputation.setup_id:
+        raise E.MismatchedSetup()
+    if accepted.party_indices() != precomputation.party_indices:
+        raise E.MismatchedCommittee()
+    if isinstance(ciphertexts, CiphertextBatch):
+        second = ciphertexts.second
+    else:
+        second = b"".join(c.second for c in ciphertexts)
+    if device_output:
+        out = empty_device(GTB * batch.batch_size())
+        _open_into(out, precomputation, accepted, batch, second, cross_terms)
+        return out
+    msgs = bytearray(GTB * batch.batch_size())
+    _open_into(msgs, precomputation, accepted, batch, second, cross_terms)
+    return [bytes(msgs[GTB * i : GTB * (i + 1)]) if batch.valid[i] else None for i in range(batch.batch_size())]
+
+
+def _open_into(out, pre, accepted, batch, second, cross_terms) -> None:
+    _ctx().call("wbte_wbtx_open", out, pre.opening_keys, b"".join(s.sigma for s in accepted.shares()),
+                accepted.party_count(), second, cross_terms.beta, batch.valid_dev, batch.batch_size())
+
+
+def decrypt(decryption_key: PublicDecryptionKey, ciphertexts: Sequence[Ciphertext],
+            shares: Sequence[DecryptionShare], rng=None) -> List[Optional[bytes]]:
+    """Convenience wrapper around all public phases (weighted_btx/src/decryption.rs:698-709)."""
+    _validate_batch_size(decryption_key, len(ciphertexts))
+    batch = validate_batch(decryption_key, ciphertexts)
+    accepted = accept_decryption_shares(decryption_key, batch, shares, rng)
+    fixed = prepare_decryption(decryption_key, accepted)
+    cross = precompute_batch(fixed, batch)
+    return open_batch(fixed, accepted, batch, ciphertexts, cross)

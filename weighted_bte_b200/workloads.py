@@ -1,0 +1,73 @@
+"""Synthetic workloads for the decryption benchmarks.
+
+No public dataset is involved: party weights, secrets and plaintexts are
+seeded synthetic inputs with the shapes of the benchmark configurations.
+
+* weighted_btx, B = 512: n = 128 parties with Zipf(s = 1) weights w_k ~ 1/k
+  scaled to W = 4096 (largest-remainder rounding, every weight >= 1);
+  a set is authorized when its weight exceeds t = floor(W / 3); the
+  committee is the heaviest-first minimal authorized set
+  (weighted_btx/examples/paper_reproduction.rs:581-607); ChaCha20 seed 1.
+* Plaintexts are uniform 32-byte strings mapped to GT as
+  Gt::generator()^(LE(bytes) mod r); the crates encrypt GT elements only.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from fractions import Fraction
+from typing import List, Tuple
+
+
+def zipf_weights(n: int, total: int, s: float = 1.0) -> List[int]:
+    """Integer weights proportional to 1/k^s summing to `total`, each >= 1."""
+    if total < n:
+        raise ValueError("total weight must be at least the party count")
+    raw = [Fraction(1, 1) / Fraction(k) ** Fraction(s).limit_denominator(1000) if s != 1.0 else Fraction(1, k)
+           for k in range(1, n + 1)]
+    norm = sum(raw)
+    quotas = [r * total / norm for r in raw]
+    base = [max(1, int(q)) for q in quotas]
+    rest = total - sum(base)
+    order = sorted(range(n), key=lambda i: (-(quotas[i] - int(quotas[i])), i))
+    i = 0
+    while rest > 0:
+        base[order[i % n]] += 1
+        rest -= 1
+        i += 1
+    while rest < 0:
+        j = max(range(n), key=lambda k: (base[k], -k))
+        base[j] -= 1
+        rest += 1
+    return base
+
+
+def minimal_authorized_parties(weights: List[int], threshold: int) -> Tuple[List[int], int]:
+    """Heaviest-first minimal committee with weight > threshold."""
+    ranked = sorted(range(len(weights)), key=lambda i: (-weights[i], i))
+    chosen, acc = [], 0
+    for i in ranked:
+        acc += weights[i]
+        chosen.append(i)
+        if acc > threshold:
+            return chosen, acc
+    raise ValueError("total weight does not exceed the threshold")
+
+
+@dataclass
+class WeightedBtxConfig:
+    name: str
+    batch_size: int
+    parties: int
+    total_weight: int
+    seed: int
+
+    @property
+    def weights(self) -> List[int]:
+        return zipf_weights(self.parties, self.total_weight)
+
+    @property
+    def threshold(self) -> int:
+        return self.total_weight // 3
+
+
+WBTX_B512 = WeightedBtxConfig("weighted_btx B=512 n=128 Zipf(1) W=4096 t=W/3", 512, 128, 4096, 1)
