@@ -58,7 +58,8 @@ int32_t wbte_version(void);
 /* One context per GPU and caller thread.  hbm_budget_bytes = 0: no limit. */
 int32_t wbte_ctx_create(int32_t device, uint64_t hbm_budget_bytes, wbte_ctx **out);
 int32_t wbte_ctx_destroy(wbte_ctx *ctx);
-/* Use a caller-owned cudaStream_t (NULL: the context's own stream). */
+/* Use a caller-owned cudaStream_t (NULL: the context's own non-blocking
+ * stream; cudaStreamLegacy to order with the legacy default stream). */
 int32_t wbte_ctx_set_stream(wbte_ctx *ctx, void *cuda_stream);
 int32_t wbte_ctx_synchronize(wbte_ctx *ctx);
 const char *wbte_ctx_last_error(const wbte_ctx *ctx);

@@ -30,6 +30,7 @@ STATUS_NAMES = {
     -7: "WBTE_ERR_INTERPOLATION",
 }
 FE_FULL, FE_EASY, FE_HARD = 0, 1, 2
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 G1_BYTES, G2_BYTES, GT_BYTES, FR_BYTES, LINE_BYTES, MILLER_LINES = 96, 192, 576, 32, 288, 68
 
 
@@ -232,7 +233,13 @@ class Context:
             pass
 
     def set_stream(self, stream_handle: int | None):
-        self.lib.wbte_ctx_set_stream(self.handle, stream_handle or None)
+        """Issue work on `stream_handle` (a cudaStream_t).  Handle 0 is the
+        legacy default stream, passed on as cudaStreamLegacy; None selects the
+        context's own stream."""
+        if stream_handle is None:
+            self.lib.wbte_ctx_set_stream(self.handle, None)
+        else:
+            self.lib.wbte_ctx_set_stream(self.handle, stream_handle if stream_handle else CUDA_STREAM_LEGACY)
 
     def synchronize(self):
         self._check(self.lib.wbte_ctx_synchronize(self.handle))
