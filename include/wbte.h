@@ -85,6 +85,25 @@ int32_t wbte_profile_read(char *names, int32_t name_stride, double *ms, int64_t 
 int32_t wbte_g1_msm(wbte_ctx *ctx, void *out, const void *points, const void *scalars, uint64_t n);
 /* Replaces blst_p2s_mult_pippenger (weighted_btx/src/blst_utils.rs:88-99). */
 int32_t wbte_g2_msm(wbte_ctx *ctx, void *out, const void *points, const void *scalars, uint64_t n);
+/* The G1 MSM of wbte_g1_msm for callers that must not allocate device
+ * memory while they serve a request -- for example a service that reserved
+ * HBM up front for its resident keys and buffers, where a new allocation
+ * could fail under memory pressure mid-request, stall on device-wide
+ * synchronisation, or fragment the partition.  It has no counterpart in the
+ * reference (blst takes caller scratch; this entry point needs none).
+ * Working memory is one fixed 8 MiB array in the library's device image,
+ * held by every GPU that loads the library until the process exits; the
+ * call allocates nothing and needs no context.
+ *   - out, points, scalars: device memory of the current device (host
+ *     pointers are rejected with WBTE_ERR_INVALID_ARG); stream: a
+ *     cudaStream_t (NULL: legacy default stream).  Asynchronous.
+ *   - n <= 16384 points; larger n returns WBTE_ERR_SIZE.
+ *   - The first call on a device looks up the array's device address (with
+ *     that device current); make that first call before any stream capture.
+ *   - Every call shares the array and it keeps the last call's contents:
+ *     calls whose work overlaps on the GPU (other streams, other threads)
+ *     race and give wrong results; serialise them on one stream. */
+int32_t wbte_g1_msm_static(void *out, const void *points, const void *scalars, uint64_t n, void *stream);
 /* k MSMs of common length n in one launch sequence:
  *   out[j] = sum_t scalars[v_j * n + t] * points[point_base[j] + idx[t]]
  * with idx = point_index (NULL: t) and v_j = scalar_vector[j] (NULL: 0).

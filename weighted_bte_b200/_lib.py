@@ -97,7 +97,8 @@ _SIGNATURES = {
 EXPORTED = sorted(
     list(_SIGNATURES)
     + ["wbte_version", "wbte_ctx_create", "wbte_ctx_destroy", "wbte_ctx_set_stream", "wbte_ctx_synchronize",
-       "wbte_ctx_last_error", "wbte_ctx_launch_count", "wbte_profile_enable", "wbte_profile_read"]
+       "wbte_ctx_last_error", "wbte_ctx_launch_count", "wbte_profile_enable", "wbte_profile_read",
+       "wbte_g1_msm_static"]
 )
 
 
@@ -160,6 +161,9 @@ def load():
             fn = getattr(lib, name)
             fn.argtypes = [_VP] + args
             fn.restype = _I32
+        # context-free, allocation-free G1 MSM: (out, points, scalars, n, stream)
+        lib.wbte_g1_msm_static.argtypes = [_VP, _VP, _VP, _U64, _VP]
+        lib.wbte_g1_msm_static.restype = _I32
         _lib = lib
         return lib
 

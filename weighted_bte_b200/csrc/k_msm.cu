@@ -21,6 +21,8 @@
 //  5. combine: Horner over windows, then conversion to affine.
 // Group addition is exact and commutative, so the result does not depend on
 // the order that atomics give terms inside a bucket.
+#include <mutex>
+
 #include "launch.h"
 #include "pairing.cuh"
 
@@ -307,3 +309,72 @@ void launch_msm_family(Group g, uint8_t* out, const uint8_t* points, const int64
 }
 
 }  // namespace wbte
+
+// ===================================================================
+// Allocation-free G1 MSM.
+//
+// Some callers must not allocate device memory while they serve a request:
+// a service that has reserved HBM up front for its resident key material
+// and its request buffers cannot let the library take more, because an
+// allocation can fail under memory pressure in the middle of a request,
+// can stall on device-wide synchronisation, and fragments a carefully
+// partitioned device.  For them, wbte_g1_msm_static runs the same Pippenger
+// kernels as wbte_g1_msm but takes its working memory from one fixed array
+// that is part of the library's device image (every GPU that loads the
+// library holds it until the process exits).
+namespace {
+constexpr size_t STATIC_MSM_BYTES = size_t(8) << 20;        // 8 MiB of scratch
+constexpr size_t STATIC_MSM_TAIL = 256;                     // holds the point-base entry
+constexpr uint64_t STATIC_MSM_MAX_POINTS = 16384;
+static __device__ __align__(256) uint8_t g_static_msm_scratch[STATIC_MSM_BYTES];
+
+std::mutex g_static_mu;
+uint8_t* g_static_addr[128] = {};
+
+bool static_is_device(const void* p) {
+    cudaPointerAttributes a;
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+}  // namespace
+
+extern "C" int32_t wbte_g1_msm_static(void* out, const void* points, const void* scalars, uint64_t n, void* stream) {
+    using namespace wbte;
+    if (n > STATIC_MSM_MAX_POINTS) return -2;  // WBTE_ERR_SIZE
+    if (!static_is_device(out) || (n > 0 && (!static_is_device(points) || !static_is_device(scalars))))
+        return -1;  // WBTE_ERR_INVALID_ARG: device pointers only
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return -5;  // WBTE_ERR_CUDA
+    uint8_t* base = nullptr;
+    {
+        // one-time set-up per device, with that device current
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (!g_static_addr[dev]) {
+            void* ptr = nullptr;
+            if (cudaGetSymbolAddress(&ptr, g_static_msm_scratch) != cudaSuccess) {
+                cudaGetLastError();
+                return -5;
+            }
+            g_static_addr[dev] = static_cast<uint8_t*>(ptr);
+        }
+        base = g_static_addr[dev];
+    }
+    if (n == 0) return cudaMemsetAsync(out, 0, G1_AFF, s) == cudaSuccess ? 0 : -5;
+    MsmPlan p = msm_plan((int64_t)n, 1);
+    size_t need = msm_family_scratch_bytes(GROUP_G1, 1, 1, (int64_t)n, p);
+    if (need > STATIC_MSM_BYTES - STATIC_MSM_TAIL) return -2;
+    // point base of the single MSM: zero (the tail of the array is reused by
+    // every call, so it is cleared here; nothing else must start at zero)
+    int64_t* pbase = reinterpret_cast<int64_t*>(base + STATIC_MSM_BYTES - STATIC_MSM_TAIL);
+    if (cudaMemsetAsync(pbase, 0, sizeof(int64_t), s) != cudaSuccess) return -5;
+    // the opt-in per-kernel profiler would create CUDA events; keep it out of this call
+    g_prof_suppress = true;
+    launch_msm_family_scratch(GROUP_G1, static_cast<uint8_t*>(out), static_cast<const uint8_t*>(points), pbase,
+                              nullptr, static_cast<const uint8_t*>(scalars), nullptr, 1, 1, (int64_t)n, p, base, s);
+    g_prof_suppress = false;
+    return cudaGetLastError() == cudaSuccess ? 0 : -5;
+}

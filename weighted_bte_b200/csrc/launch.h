@@ -17,6 +17,7 @@ inline void note_launch(uint64_t k = 1) { g_launches.fetch_add(k, std::memory_or
 
 // Optional per-kernel timing: while profiling is enabled, a ProfScope records
 // CUDA events around the launches in its scope, tagged with a kernel name.
+extern thread_local bool g_prof_suppress;  // set while no events may be created
 void prof_begin(const char* tag, cudaStream_t s, void** token);
 void prof_end(void* token, cudaStream_t s);
 struct ProfScope {

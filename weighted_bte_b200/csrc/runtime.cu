@@ -28,9 +28,11 @@ std::vector<ProfRec> g_prof;
 std::atomic<bool> g_prof_on{false};
 }  // namespace
 
+thread_local bool g_prof_suppress = false;
+
 void prof_begin(const char* tag, cudaStream_t s, void** token) {
     *token = nullptr;
-    if (!g_prof_on.load(std::memory_order_relaxed)) return;
+    if (g_prof_suppress || !g_prof_on.load(std::memory_order_relaxed)) return;
     ProfRec* r = new ProfRec{tag, nullptr, nullptr};
     cudaEventCreate(&r->a);
     cudaEventCreate(&r->b);
