@@ -17,7 +17,7 @@ import threading
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "libwbte.so")
+LIB_PATH = os.environ.get("WBTE_LIB") or os.path.join(PKG, "libwbte.so")
 
 WBTE_OK = 0
 STATUS_NAMES = {

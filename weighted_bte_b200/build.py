@@ -26,6 +26,11 @@ LIB = os.path.join(PKG, "libwbte.so")
 SOURCES = ["k_arith.cu", "k_msm.cu", "k_pairing.cu", "runtime.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INCLUDE]
+# Code-layout variant of the shipped library (see fields.cuh): one out-of-line
+# copy of the Fp and of the Fp2 product.  Measured on B200 (weighted_btx,
+# B = 512): 2.5x the throughput of fully inlined arithmetic, whose hot loops
+# overflow the instruction cache (ncu: "no instruction" stalls dominate).
+DEFAULT_DEFINES: list = ["WBTE_FP_NOINLINE", "WBTE_FP2_NOINLINE"]
 
 
 def nvcc() -> str:
@@ -62,36 +67,54 @@ def _compile(src: str, digest: str, force: bool) -> str:
     return obj
 
 
-def build(force: bool = False, verbose: bool = True) -> str:
+def build(force: bool = False, verbose: bool = True, defines=None, lib_path: str = None) -> str:
+    """Compile and link.  `defines` (e.g. ["WBTE_FP_NOINLINE"]) select code-layout
+    variants; `lib_path` names the output (default: weighted_bte_b200/libwbte.so)."""
+    global FLAGS, BUILD
     if not os.path.exists(os.path.join(CSRC, "field_asm.cuh")) or force:
         subprocess.run([sys.executable, os.path.join(CSRC, "gen_field.py")], check=True)
-    os.makedirs(BUILD, exist_ok=True)
-    digest = _headers_digest()
-    with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, digest, force), SOURCES))
-    stamp = hashlib.sha256("".join(objs).encode()).hexdigest()
-    stamp_file = os.path.join(BUILD, "link.stamp")
-    if os.path.exists(LIB) and os.path.exists(stamp_file) and not force:
-        with open(stamp_file) as f:
-            if f.read() == stamp:
-                return LIB
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB + ".tmp"] + objs + ["-cudart", "static"]
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        raise RuntimeError(f"link failed:\n{res.stderr[-6000:]}")
-    os.replace(LIB + ".tmp", LIB)
-    with open(stamp_file, "w") as f:
-        f.write(stamp)
-    # drop objects of older source versions
-    keep = set(objs)
-    for name in os.listdir(BUILD):
-        p = os.path.join(BUILD, name)
-        if name.endswith(".o") and p not in keep:
-            os.remove(p)
+    defines = DEFAULT_DEFINES if defines is None else list(defines)
+    lib = lib_path or LIB
+    saved = (FLAGS, BUILD)
+    FLAGS = FLAGS + [f"-D{d}" for d in defines]
+    BUILD = os.path.join(PKG, "_build", "-".join(defines) or "base")
+    try:
+        os.makedirs(BUILD, exist_ok=True)
+        digest = _headers_digest()
+        with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+            objs = list(ex.map(lambda s: _compile(s, digest, force), SOURCES))
+        stamp = hashlib.sha256(("".join(objs) + lib).encode()).hexdigest()
+        stamp_file = os.path.join(BUILD, "link.stamp")
+        if os.path.exists(lib) and os.path.exists(stamp_file) and not force:
+            with open(stamp_file) as f:
+                if f.read() == stamp:
+                    return lib
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", lib + ".tmp"] + objs + ["-cudart", "static"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"link failed:\n{res.stderr[-6000:]}")
+        os.replace(lib + ".tmp", lib)
+        with open(stamp_file, "w") as f:
+            f.write(stamp)
+        # drop objects of older source versions
+        keep = set(objs)
+        for name in os.listdir(BUILD):
+            p = os.path.join(BUILD, name)
+            if name.endswith(".o") and p not in keep:
+                os.remove(p)
+    finally:
+        FLAGS, BUILD = saved
     if verbose:
-        print(f"built {LIB}")
-    return LIB
+        print(f"built {lib}")
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv)
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--define", action="append", default=None)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    build(force=a.force, defines=a.define, lib_path=a.out)

@@ -24,8 +24,16 @@ struct Fp12 { Fp6 c0, c1; };
 // ------------------------------------------------------------------ Fp
 WBTE_INL Fp fp_zero() { Fp r; _Pragma("unroll") for (int i = 0; i < 12; i++) r.v[i] = 0; return r; }
 WBTE_INL Fp fp_one() { Fp r; _Pragma("unroll") for (int i = 0; i < 12; i++) r.v[i] = C_FP_ONE[i]; return r; }
+#if defined(WBTE_FP_NOINLINE)
+// One out-of-line copy of the 12-limb product keeps every kernel's hot loop
+// inside the instruction cache.
+static __device__ __noinline__ Fp fp_mul_ool(Fp a, Fp b) { Fp r; fp_mont_mul(r.v, a.v, b.v); return r; }
+WBTE_INL Fp fp_mul(const Fp& a, const Fp& b) { return fp_mul_ool(a, b); }
+WBTE_INL Fp fp_sqr(const Fp& a) { return fp_mul_ool(a, a); }
+#else
 WBTE_INL Fp fp_mul(const Fp& a, const Fp& b) { Fp r; fp_mont_mul(r.v, a.v, b.v); return r; }
 WBTE_INL Fp fp_sqr(const Fp& a) { Fp r; fp_mont_mul(r.v, a.v, a.v); return r; }
+#endif
 WBTE_INL Fp fp_add(const Fp& a, const Fp& b) { Fp r; fp_add_raw(r.v, a.v, b.v); return r; }
 WBTE_INL Fp fp_sub(const Fp& a, const Fp& b) { Fp r; fp_sub_raw(r.v, a.v, b.v); return r; }
 // a + b without reduction: only valid as a multiplication input (< 2p).
@@ -98,15 +106,20 @@ WBTE_INL Fp2 fp2_neg(const Fp2& a) { return Fp2{fp_neg(a.c0), fp_neg(a.c1)}; }
 WBTE_INL Fp2 fp2_conj(const Fp2& a) { return Fp2{a.c0, fp_neg(a.c1)}; }
 WBTE_INL bool fp2_is_zero(const Fp2& a) { return fp_is_zero(a.c0) && fp_is_zero(a.c1); }
 WBTE_INL bool fp2_eq(const Fp2& a, const Fp2& b) { return fp_eq(a.c0, b.c0) && fp_eq(a.c1, b.c1); }
+#if defined(WBTE_FP2_NOINLINE)
+#define WBTE_FP2_MUL static __device__ __noinline__
+#else
+#define WBTE_FP2_MUL WBTE_INL
+#endif
 // Karatsuba: 3 Fp products; the operand sums stay unreduced (< 2p).
-WBTE_INL Fp2 fp2_mul(const Fp2& a, const Fp2& b) {
+WBTE_FP2_MUL Fp2 fp2_mul(const Fp2& a, const Fp2& b) {
     Fp t0 = fp_mul(a.c0, b.c0);
     Fp t1 = fp_mul(a.c1, b.c1);
     Fp t2 = fp_mul(fp_add_lazy(a.c0, a.c1), fp_add_lazy(b.c0, b.c1));
     return Fp2{fp_sub(t0, t1), fp_sub(fp_sub(t2, t0), t1)};
 }
 // (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
-WBTE_INL Fp2 fp2_sqr(const Fp2& a) {
+WBTE_FP2_MUL Fp2 fp2_sqr(const Fp2& a) {
     Fp t = fp_mul(a.c0, a.c1);
     Fp c0 = fp_mul(fp_add_lazy(a.c0, a.c1), fp_sub(a.c0, a.c1));
     return Fp2{c0, fp_dbl(t)};
