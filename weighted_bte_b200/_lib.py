@@ -274,12 +274,18 @@ class Context:
         return keep
 
 
-_default = {}
+_default = threading.local()
 
 
 def default_context(device: int = 0) -> Context:
-    ctx = _default.get(device)
+    """The calling thread's context on `device`.  Contexts are per thread so
+    that threads working on separate streams never share a context's stream
+    setting or error state."""
+    table = getattr(_default, "table", None)
+    if table is None:
+        table = _default.table = {}
+    ctx = table.get(device)
     if ctx is None:
         ctx = Context(device)
-        _default[device] = ctx
+        table[device] = ctx
     return ctx

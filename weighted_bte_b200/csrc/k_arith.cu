@@ -1,5 +1,7 @@
 // Scalar-field kernels, batched point multiplication, radix-2 group
 // transforms, compressed encodings and Schnorr checks.
+#include <mutex>
+
 #include "launch.h"
 #include "pairing.cuh"
 
@@ -199,22 +201,58 @@ __global__ void k_ntt_load(uint8_t* work, const uint8_t* in, int64_t n, int bits
     store_vec(reinterpret_cast<Xyzz<F>*>(work) + bitrev64(i, bits), p);
 }
 
-// one radix-2 butterfly per thread; twiddle index j * (n / size)
+// One radix-2 butterfly per group of L lanes (blocks of one warp); twiddle
+// index j * (n / size).  The twiddle multiplication is split along the
+// base-|x| digits of the twiddle: four lanes on G2 ([d_c] (-1)^c psi^c(v)),
+// two lanes on G1 ([a]v and [b](phi(v) + v)); the parts are summed in shared
+// memory before the butterfly.
+template <class F> struct NttLanes;
+template <> struct NttLanes<Fp> { static constexpr int L = 2; };
+template <> struct NttLanes<Fp2> { static constexpr int L = 4; };
+constexpr int WARP = 32;
+
+WBTE_INL void ntt_part(G1X& out, const G1X& v, const uint64_t d[4], int c) { g1_mul_lane(out, v, d, c); }
+WBTE_INL void ntt_part(G2X& out, const G2X& v, const uint64_t d[4], int c) { g2_mul_lane(out, v, d, c); }
+
 template <class F>
-__global__ void k_ntt_stage(uint8_t* work, const uint8_t* tw, int64_t n, int64_t half) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n / 2) return;
-    int64_t chunk = t / half, j = t % half;
+__global__ void __launch_bounds__(WARP) k_ntt_stage(uint8_t* work, const uint8_t* tw, int64_t n, int64_t half) {
+    constexpr int L = NttLanes<F>::L;
+    __shared__ Xyzz<F> sh[WARP];
+    const int lane = threadIdx.x, c = lane % L;
+    const int64_t t = ((int64_t)blockIdx.x * WARP + lane) / L;
+    const bool active = t < n / 2;
+    const int64_t chunk = active ? t / half : 0, j = active ? t % half : 0;
+    const int64_t a = chunk * 2 * half + j, b = a + half;
     Xyzz<F>* w = reinterpret_cast<Xyzz<F>*>(work);
-    int64_t a = chunk * 2 * half + j, b = a + half;
-    Xyzz<F> u = load_vec(w + a), v = load_vec(w + b);
-    if (j != 0) {
-        uint32_t k[8];
-        load_scalar(k, tw + FR_SZ * (j * (n / (2 * half))));
-        v = xyzz_mul(v, k);
+    Xyzz<F> part;
+    set_inf(part);
+    if (active) {
+        Xyzz<F> v = load_vec(w + b);
+        if (j != 0) {
+            uint32_t s[8];
+            load_scalar(s, tw + FR_SZ * (j * (n / (2 * half))));
+            uint64_t d[4];
+            decompose_base_x(d, s);
+            ntt_part(part, v, d, c);
+        } else if (c == 0) {
+            part = v;
+        }
     }
-    store_vec(w + a, xyzz_add(u, v));
-    store_vec(w + b, xyzz_add(u, neg(v)));
+    store_vec(sh + lane, part);
+    __syncwarp();
+    for (int step = 1; step < L; step *= 2) {
+        if (c % (2 * step) == 0) store_vec(sh + lane, xyzz_add(load_vec(sh + lane), load_vec(sh + lane + step)));
+        __syncwarp();
+    }
+    // lanes 0 and 1 both read u before either output is written
+    Xyzz<F> u;
+    if (active && c < 2) u = load_vec(w + a);
+    __syncwarp();
+    if (active && c < 2) {
+        Xyzz<F> tv = load_vec(sh + (lane - c));
+        if (c == 1) tv = neg(tv);
+        store_vec(w + (c == 0 ? a : b), xyzz_add(u, tv));
+    }
 }
 
 template <class F>
@@ -383,22 +421,30 @@ void launch_mul_batch(Group g, uint8_t* out, const uint8_t* pts, int64_t stride,
     else k_mul_batch<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, pts, stride, scalars, n);
 }
 
-// generator tables are built once per device on first use
+// Generator tables are built once per device on first use.  The build is
+// finished (stream synchronised) before the table is published, so callers
+// on other streams never read a table still being written.
 static uint8_t* g_gen_table[2][64] = {};
+static std::mutex g_gen_mu;
 void launch_mul_generator(Group g, uint8_t* out, const uint8_t* scalars, int64_t n, cudaStream_t s) {
     ProfScope prof_("mul_generator", s);
     if (n <= 0) return;
     int dev = 0;
     cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return;
     int gi = g == GROUP_G1 ? 0 : 1;
     size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
-    if (!g_gen_table[gi][dev]) {
-        uint8_t* t = nullptr;
-        if (cudaMalloc(&t, aff * 256 * 32) != cudaSuccess) return;
-        note_launch();
-        if (g == GROUP_G1) k_build_gen_table<Fp><<<32, 256, 0, s>>>(t);
-        else k_build_gen_table<Fp2><<<32, 256, 0, s>>>(t);
-        g_gen_table[gi][dev] = t;
+    {
+        std::lock_guard<std::mutex> lock(g_gen_mu);
+        if (!g_gen_table[gi][dev]) {
+            uint8_t* t = nullptr;
+            if (cudaMalloc(&t, aff * 256 * 32) != cudaSuccess) return;
+            note_launch();
+            if (g == GROUP_G1) k_build_gen_table<Fp><<<32, 256, 0, s>>>(t);
+            else k_build_gen_table<Fp2><<<32, 256, 0, s>>>(t);
+            if (cudaStreamSynchronize(s) != cudaSuccess) return;
+            g_gen_table[gi][dev] = t;
+        }
     }
     note_launch();
     if (g == GROUP_G1) k_mul_generator<Fp><<<blocks_for(n), TPB, 0, s>>>(out, g_gen_table[gi][dev], scalars, n);
@@ -436,7 +482,7 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
         k_ntt_load<Fp><<<blocks_for(n), TPB, 0, s>>>(work, io, n, bits);
         for (int64_t half = 1; half < n; half *= 2) {
             note_launch();
-            k_ntt_stage<Fp><<<blocks_for(n / 2, 64), 64, 0, s>>>(work, tw, n, half);
+            k_ntt_stage<Fp><<<blocks_for(NttLanes<Fp>::L * (n / 2), WARP), WARP, 0, s>>>(work, tw, n, half);
         }
         note_launch();
         k_xyzz_to_affine<Fp><<<blocks_for(n), TPB, 0, s>>>(io, work, n);
@@ -445,7 +491,7 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
         k_ntt_load<Fp2><<<blocks_for(n), TPB, 0, s>>>(work, io, n, bits);
         for (int64_t half = 1; half < n; half *= 2) {
             note_launch();
-            k_ntt_stage<Fp2><<<blocks_for(n / 2, 64), 64, 0, s>>>(work, tw, n, half);
+            k_ntt_stage<Fp2><<<blocks_for(NttLanes<Fp2>::L * (n / 2), WARP), WARP, 0, s>>>(work, tw, n, half);
         }
         note_launch();
         k_xyzz_to_affine<Fp2><<<blocks_for(n), TPB, 0, s>>>(io, work, n);

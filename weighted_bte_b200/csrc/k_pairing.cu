@@ -87,56 +87,99 @@ __global__ void k_gt_bitrev(uint8_t* dst, const uint8_t* src, int64_t n, int bit
     store_vec(as_gt(dst) + bitrev64(i, bits), load_vec(as_gt(src) + i));
 }
 
-// One butterfly per thread: u' = u * t, v' = u * t^-1 with t = v^tw (decomposed
-// action; inverse by conjugation in the cyclotomic subgroup).
-__global__ void k_gt_stage(uint8_t* io, const uint8_t* tw, int64_t n, int64_t half) {
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n / 2) return;
-    int64_t chunk = t / half, j = t % half;
-    int64_t a = chunk * 2 * half + j, b = a + half;
-    Fp12 u = load_vec(as_gt(io) + a), v = load_vec(as_gt(io) + b);
-    Fp12 tv;
-    if (j != 0) {
-        uint32_t s[8];
-        load_scalar(s, tw + FR_SZ * (j * (n / (2 * half))));
-        gt_pow(tv, v, s);
-    } else {
-        tv = v;
+// The GT transforms and GT exponentiation split each exponentiation v^s over
+// GT_LANES = 4 consecutive threads, one base-|x| digit of s each
+// (gt_pow_lane); the four parts meet in shared memory.  Blocks are one warp.
+constexpr int GT_LANES = 4;
+constexpr int WARP = 32;
+
+// parts of v^s for the butterfly or element this lane belongs to
+WBTE_INL void gt_pow_part(Fp12& part, const Fp12& v, const uint8_t* scalar, int c) {
+    uint32_t s[8];
+    load_scalar(s, scalar);
+    uint64_t d[4];
+    decompose_base_x(d, s);
+    gt_pow_lane(part, v, d[c], c);
+}
+
+// sh[lane - c] <- product of the four parts of its group
+WBTE_INL void gt_combine(Fp12* sh, int lane, int c) {
+    __syncwarp();
+    if ((c & 1) == 0) {
+        Fp12 x = load_vec(sh + lane), y = load_vec(sh + lane + 1);
+        fp12_mul(x, x, y);
+        store_vec(sh + lane, x);
     }
-    Fp12 x, y, ti;
-    fp12_mul(x, u, tv);
-    fp12_conj(ti, tv);
-    fp12_mul(y, u, ti);
-    store_vec(as_gt(io) + a, x);
-    store_vec(as_gt(io) + b, y);
+    __syncwarp();
+    if (c == 0) {
+        Fp12 x = load_vec(sh + lane), y = load_vec(sh + lane + 2);
+        fp12_mul(x, x, y);
+        store_vec(sh + lane, x);
+    }
+    __syncwarp();
+}
+
+// One butterfly per group of lanes: u' = u t, v' = u t^-1 with t = v^tw
+// (inverse by conjugation in the cyclotomic subgroup).
+__global__ void __launch_bounds__(WARP) k_gt_stage(uint8_t* io, const uint8_t* tw, int64_t n, int64_t half) {
+    __shared__ Fp12 sh[WARP];
+    const int lane = threadIdx.x, c = lane % GT_LANES;
+    const int64_t t = ((int64_t)blockIdx.x * WARP + lane) / GT_LANES;
+    const bool active = t < n / 2;
+    const int64_t chunk = active ? t / half : 0, j = active ? t % half : 0;
+    const int64_t a = chunk * 2 * half + j, b = a + half;
+    Fp12 part = fp12_one();
+    if (active) {
+        Fp12 v = load_vec(as_gt(io) + b);
+        if (j != 0) gt_pow_part(part, v, tw + FR_SZ * (j * (n / (2 * half))), c);
+        else if (c == 0) part = v;
+    }
+    store_vec(sh + lane, part);
+    gt_combine(sh, lane, c);
+    // lanes 0 and 1 both read u before either output is written
+    Fp12 u;
+    if (active && c < 2) u = load_vec(as_gt(io) + a);
+    __syncwarp();
+    if (active && c < 2) {
+        Fp12 tv = load_vec(sh + (lane - c)), r;
+        if (c == 1) fp12_conj(tv, tv);
+        fp12_mul(r, u, tv);
+        store_vec(as_gt(io) + (c == 0 ? a : b), r);
+    }
 }
 
 // last stage keeping only the first out_count outputs
-__global__ void k_gt_last_prefix(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count) {
-    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (j >= out_count) return;
-    int64_t half = n / 2;
-    Fp12 u = load_vec(as_gt(io) + j), v = load_vec(as_gt(io) + half + j);
-    Fp12 tv;
-    if (j != 0) {
-        uint32_t s[8];
-        load_scalar(s, tw + FR_SZ * j);
-        gt_pow(tv, v, s);
-    } else {
-        tv = v;
+__global__ void __launch_bounds__(WARP) k_gt_last_prefix(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count) {
+    __shared__ Fp12 sh[WARP];
+    const int lane = threadIdx.x, c = lane % GT_LANES;
+    const int64_t j = ((int64_t)blockIdx.x * WARP + lane) / GT_LANES;
+    const bool active = j < out_count;
+    const int64_t half = n / 2;
+    Fp12 part = fp12_one();
+    if (active) {
+        Fp12 v = load_vec(as_gt(io) + half + j);
+        if (j != 0) gt_pow_part(part, v, tw + FR_SZ * j, c);
+        else if (c == 0) part = v;
     }
-    fp12_mul(u, u, tv);
-    store_vec(as_gt(io) + j, u);
+    store_vec(sh + lane, part);
+    gt_combine(sh, lane, c);
+    if (active && c == 0) {
+        Fp12 u = load_vec(as_gt(io) + j), tv = load_vec(sh + lane);
+        fp12_mul(u, u, tv);
+        store_vec(as_gt(io) + j, u);
+    }
 }
 
-__global__ void k_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint8_t* scalars, int64_t n) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Fp12 b = load_vec(as_gt(base) + stride * i), r;
-    uint32_t s[8];
-    load_scalar(s, scalars + FR_SZ * i);
-    gt_pow(r, b, s);
-    store_vec(as_gt(out) + i, r);
+__global__ void __launch_bounds__(WARP) k_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint8_t* scalars, int64_t n) {
+    __shared__ Fp12 sh[WARP];
+    const int lane = threadIdx.x, c = lane % GT_LANES;
+    const int64_t i = ((int64_t)blockIdx.x * WARP + lane) / GT_LANES;
+    const bool active = i < n;
+    Fp12 part = fp12_one();
+    if (active) gt_pow_part(part, load_vec(as_gt(base) + stride * i), scalars + FR_SZ * i, c);
+    store_vec(sh + lane, part);
+    gt_combine(sh, lane, c);
+    if (active && c == 0) store_vec(as_gt(out) + i, load_vec(sh + lane));
 }
 
 __global__ void k_fp12_mul(uint8_t* out, const uint8_t* a, int64_t sa, const uint8_t* b, int64_t sb, bool conj_b, int64_t n) {
@@ -254,11 +297,11 @@ static void gt_transform(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_
     int64_t last_half = prefix ? n / 4 : n / 2;
     for (int64_t half = 1; half <= last_half; half *= 2) {
         note_launch();
-        k_gt_stage<<<blocks_for(n / 2), TPB, 0, s>>>(tmp, tw, n, half);
+        k_gt_stage<<<blocks_for(GT_LANES * (n / 2), WARP), WARP, 0, s>>>(tmp, tw, n, half);
     }
     if (prefix && out_count > 0) {
         note_launch();
-        k_gt_last_prefix<<<blocks_for(out_count), TPB, 0, s>>>(tmp, tw, n, out_count);
+        k_gt_last_prefix<<<blocks_for(GT_LANES * out_count, WARP), WARP, 0, s>>>(tmp, tw, n, out_count);
     }
     cudaMemcpyAsync(io, tmp, GT_SZ * (size_t)n, cudaMemcpyDeviceToDevice, s);
     cudaFreeAsync(tmp, s);
@@ -272,7 +315,7 @@ void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint
     ProfScope prof_("gt_pow", s);
     if (n <= 0) return;
     note_launch();
-    k_gt_pow<<<blocks_for(n), TPB, 0, s>>>(out, base, stride, scalars, n);
+    k_gt_pow<<<blocks_for(GT_LANES * n, WARP), WARP, 0, s>>>(out, base, stride, scalars, n);
 }
 void launch_fp12_mul(uint8_t* out, const uint8_t* a, int64_t sa, const uint8_t* b, int64_t sb, bool conj_b, int64_t n, cudaStream_t s) {
     if (n <= 0) return;

@@ -266,4 +266,151 @@ WBTE_INL void gt_pow(Fp12& out, const Fp12& value, const uint32_t s[8]) {
     cyc_pow_plan(out, value, pl);
 }
 
+// ------------------------------------------------ lane-split exponentiation
+// The transforms split one exponentiation across a few threads of a warp, one
+// base-|x| digit each, so that every thread of the warp runs the same fixed
+// schedule of squarings (data-dependent NAF lengths otherwise diverge).
+
+// s = d0 + d1|x| + d2|x|^2 + d3|x|^3 with 0 <= dc < |x| (s < r < |x|^4)
+WBTE_INL void decompose_base_x(uint64_t d[4], const uint32_t s_in[8]) {
+    uint32_t s[8];
+    _Pragma("unroll") for (int i = 0; i < 8; i++) s[i] = s_in[i];
+    for (int c = 0; c < 4; c++) {
+        uint32_t lo16 = s[0] & 0xffffu;
+        uint16_t chunks[15];
+        for (int j = 0; j < 15; j++) {
+            int bit = 16 + 16 * j;
+            chunks[j] = (uint16_t)(s[bit >> 5] >> (bit & 31));
+        }
+        uint64_t rem = 0;
+        uint16_t q[15];
+        for (int j = 14; j >= 0; j--) {
+            uint64_t cur = (rem << 16) | chunks[j];
+            q[j] = (uint16_t)(cur / X_ODD);
+            rem = cur % X_ODD;
+        }
+        d[c] = (rem << 16) | lo16;
+        for (int i = 0; i < 8; i++) s[i] = 0;
+        for (int j = 0; j < 15; j++) s[j >> 1] |= (uint32_t)q[j] << (16 * (j & 1));
+    }
+}
+
+// Signed radix-16 recoding of v = hi 2^64 + lo with `top` nibbles (16 or 32):
+// v = sum_{k=0..top} digit_k 16^k with digits in [-7, 8].  Rounding a nibble
+// above 8 down by 16 carries one into the next digit, and the carry into
+// digit k is set exactly when the low k nibbles of v exceed 0x88...8 (k
+// eights), so each digit is computed on its own, without a digit array.
+WBTE_INL int r16_carry(uint64_t lo, uint64_t hi, int k) {
+    constexpr uint64_t E = 0x8888888888888888ull;
+    if (k <= 16) {
+        uint64_t m = k == 16 ? ~0ull : ((1ull << (4 * k)) - 1);
+        return (lo & m) > (E & m);
+    }
+    int kh = k - 16;
+    uint64_t m = kh == 16 ? ~0ull : ((1ull << (4 * kh)) - 1);
+    uint64_t h = hi & m, e = E & m;
+    return h > e || (h == e && lo > E);
+}
+WBTE_INL int r16_digit(uint64_t lo, uint64_t hi, int k, int top) {
+    int nib = 0;
+    if (k < top) nib = (int)(((k < 16) ? (lo >> (4 * k)) : (hi >> (4 * (k - 16)))) & 15u);
+    int cout = k < top ? r16_carry(lo, hi, k + 1) : 0;
+    return nib + r16_carry(lo, hi, k) - 16 * cout;
+}
+
+// out = (+-Frobenius^c(v))^d for one base-|x| digit d (conjugated for odd
+// c), i.e. v^(d |x|^c) on GT; v must be cyclotomic.
+static __device__ __noinline__ void gt_pow_lane(Fp12& out, const Fp12& v, uint64_t d, int c) {
+    Fp12 tab[8];  // base^1 .. base^8
+    if (c == 0) {
+        tab[0] = v;
+    } else {
+        fp12_frobenius(tab[0], v, c);
+        if (c & 1) fp12_conj(tab[0], tab[0]);
+    }
+    fp12_cyclotomic_sqr(tab[1], tab[0]);
+    for (int k = 2; k < 8; k++) fp12_mul(tab[k], tab[k - 1], tab[0]);
+    Fp12 acc = fp12_one();
+    for (int k = 16; k >= 0; k--) {
+        if (k != 16) {
+            fp12_cyclotomic_sqr(acc, acc);
+            fp12_cyclotomic_sqr(acc, acc);
+            fp12_cyclotomic_sqr(acc, acc);
+            fp12_cyclotomic_sqr(acc, acc);
+        }
+        int dd = r16_digit(d, 0, k, 16);
+        int ad = dd < 0 ? -dd : dd;
+        if (ad) {
+            Fp12 m = tab[ad - 1];
+            if (dd < 0) fp12_conj(m, m);
+            fp12_mul(acc, acc, m);
+        }
+    }
+    out = acc;
+}
+
+// out = [w]p for w = hi 2^64 + lo < 16^top, over the signed radix-16 digits
+template <class F>
+static __device__ __noinline__ void xyzz_mul_r16(Xyzz<F>& out, const Xyzz<F>& p, uint64_t lo, uint64_t hi, int top) {
+    Xyzz<F> tab[8];  // [1]p .. [8]p
+    tab[0] = p;
+    tab[1] = xyzz_dbl(tab[0]);
+    for (int k = 2; k < 8; k++) tab[k] = xyzz_add(tab[k - 1], tab[0]);
+    Xyzz<F> acc;
+    set_inf(acc);
+    for (int k = top; k >= 0; k--) {
+        acc = xyzz_dbl(acc);
+        acc = xyzz_dbl(acc);
+        acc = xyzz_dbl(acc);
+        acc = xyzz_dbl(acc);
+        int dd = r16_digit(lo, hi, k, top);
+        int ad = dd < 0 ? -dd : dd;
+        if (ad) {
+            Xyzz<F> m = tab[ad - 1];
+            if (dd < 0) m = neg(m);
+            acc = xyzz_add(acc, m);
+        }
+    }
+    out = acc;
+}
+
+// psi (untwist-Frobenius-twist) on G2 in XYZZ coordinates; acts as [x]
+WBTE_INL G2X g2_psi(const G2X& p) {
+    G2X r;
+    r.X = fp2_mul(fp2_conj(p.X), fp2_from_const(C_PSI_CX));
+    r.Y = fp2_mul(fp2_conj(p.Y), fp2_from_const(C_PSI_CY));
+    r.ZZ = fp2_conj(p.ZZ);
+    r.ZZZ = fp2_conj(p.ZZZ);
+    return r;
+}
+// phi (x, y) -> (beta x, y) on G1 in XYZZ coordinates; acts as [x^2 - 1]
+WBTE_INL G1X g1_phi(const G1X& p) {
+    G1X r = p;
+    r.X = fp_mul(p.X, fp_from_const(C_GLV_BETA));
+    return r;
+}
+
+// Lane c (0..3) of [s]v on G2 for s = sum_c d_c |x|^c:
+// out = [d_c]((-1)^c psi^c(v)) = [d_c |x|^c]v.
+WBTE_INL void g2_mul_lane(G2X& out, const G2X& v, const uint64_t d[4], int c) {
+    G2X base = v;
+    for (int i = 0; i < c; i++) base = g2_psi(base);
+    if (c & 1) base = neg(base);
+    xyzz_mul_r16(out, base, d[c], 0, 16);
+}
+
+// Lane c (0 or 1) of [s]v on G1 for s = a + b |x|^2 with a = d0 + d1|x| and
+// b = d2 + d3|x| (both below |x|^2 < 2^128): [a]v, or [b](phi(v) + v) since
+// phi(v) + v = [x^2]v.
+WBTE_INL void g1_mul_lane(G1X& out, const G1X& v, const uint64_t d[4], int c) {
+    G1X base = v;
+    if (c) base = xyzz_add(g1_phi(v), v);
+    uint64_t lo = d[2 * c], hi = d[2 * c + 1];
+    // w = lo + hi |x| as a 128-bit integer
+    uint64_t plo = hi * X_ABS, phi = __umul64hi(hi, X_ABS);
+    uint64_t wlo = plo + lo;
+    uint64_t whi = phi + (wlo < plo ? 1 : 0);
+    xyzz_mul_r16(out, base, wlo, whi, 32);
+}
+
 }  // namespace wbte
