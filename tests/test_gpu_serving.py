@@ -1,0 +1,85 @@
+"""Served and batched decryption: every request's result is byte-identical
+whether it runs alone (the plain `decrypt` path) or in a mix of concurrent
+requests of different batch sizes and committees, with and without the
+committee cache, and admission respects the HBM budget."""
+import pytest
+
+from weighted_bte_b200 import serving
+from weighted_bte_b200 import weighted_btx as wb
+from weighted_bte_b200.rng import ChaCha20Rng
+
+pytestmark = pytest.mark.gpu
+
+WEIGHTS, THRESHOLD, MAX_BATCH = [1, 3, 2, 4, 1], 5, 8
+
+
+@pytest.fixture(scope="module")
+def mix():
+    mat = wb.keygen_with_rng(wb.KeygenConfig(MAX_BATCH, WEIGHTS, THRESHOLD), ChaCha20Rng.seed_from_u64(41))
+    rng = ChaCha20Rng.seed_from_u64(42)
+    # (batch size, committee): uneven sizes, two committees, repeated contexts
+    shapes = [(8, [1, 3]), (3, [1, 3]), (5, [0, 2, 3]), (8, [1, 3]), (1, [3, 4, 0]), (6, [0, 2, 3]), (8, [1, 3])]
+    reqs = []
+    for B, parties in shapes:
+        msgs = wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(B)])
+        cts = wb.encrypt_many(mat.encryption_key, msgs, rng)
+        keys = [mat.party_keys[j] for j in sorted(parties)]
+        reqs.append((cts, keys, msgs))
+    # one ciphertext with a broken proof: its slot decrypts to None
+    cts, keys, msgs = reqs[2]
+    bad = cts[1]
+    cts[1] = wb.Ciphertext(bad.first, bad.second, wb.SchnorrProof(bad.proof.commitment, (bad.proof.response + 1) % wb.R))
+    return mat, reqs
+
+
+def alone(mat, cts, keys):
+    batch = wb.validate_batch(mat.decryption_key, cts)
+    shares = wb.partial_decrypt_many(keys, batch)
+    return wb.decrypt(mat.decryption_key, cts, shares, ChaCha20Rng.seed_from_u64(5))
+
+
+def test_results_identical_alone_and_in_the_mix(mix):
+    mat, reqs = mix
+    solo = [alone(mat, cts, keys) for cts, keys, _ in reqs]
+    for (cts, _, msgs), out in zip(reqs, solo):
+        assert [o for o in out if o is not None] == [m for m, o in zip(msgs, out) if o is not None]
+    assert solo[2][1] is None and sum(o is None for r in solo for o in r) == 1
+    for cache in (True, False):
+        with serving.DecryptionServer(mat.decryption_key, slots=3, cache_committees=cache) as srv:
+            futs = [srv.submit(cts, keys, seed=i) for i, (cts, keys, _) in enumerate(reqs)]
+            mixed = [f.result() for f in futs]
+            st = srv.stats()
+        assert mixed == solo
+        assert st["requests"] == len(reqs) and st["p50_ms"] is not None and st["p99_ms"] >= st["p50_ms"]
+        if cache:
+            # three distinct (batch size, committee) contexts repeat: 8/[1,3] three times
+            assert st["cache_misses"] == 5 and st["cache_hits"] == 2
+
+
+def test_budget_admits_one_request_at_a_time(mix):
+    mat, reqs = mix
+    sizes = [serving.request_bytes(len(c), len(k)) + serving.preparation_bytes(
+        len(c), len(k), sum(mat.decryption_key.party_weight(x.party_index) for x in k)) for c, k, _ in reqs]
+    budget = max(sizes)  # the largest request never shares the GPU with another
+    with serving.DecryptionServer(mat.decryption_key, slots=4, hbm_budget_bytes=budget) as srv:
+        futs = [srv.submit(cts, keys) for cts, keys, _ in reqs]
+        out = [f.result() for f in futs]
+        st = srv.stats()
+    assert out == [alone(mat, cts, keys) for cts, keys, _ in reqs]
+    assert st["peak_bytes"] <= budget and st["peak_in_flight"] < len(reqs)
+    with serving.DecryptionServer(mat.decryption_key, slots=2, hbm_budget_bytes=min(sizes) - 1) as srv:
+        with pytest.raises(MemoryError):
+            srv.submit(reqs[0][0], reqs[0][1])
+
+
+def test_concurrent_streams_match_sequential(mix):
+    mat, reqs = mix
+    cache = serving.CommitteeCache(1 << 30)
+
+    def fn(r):
+        cts, keys, _ = r
+        return serving.decrypt_request(mat.decryption_key, cts, keys, ChaCha20Rng.seed_from_u64(1), cache)
+
+    outs, ms = serving.run_concurrent(fn, reqs, 4)
+    assert ms > 0
+    assert outs == [alone(mat, cts, keys) for cts, keys, _ in reqs]
