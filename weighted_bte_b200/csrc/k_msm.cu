@@ -21,6 +21,9 @@
 //  5. combine: Horner over windows, then conversion to affine.
 // Group addition is exact and commutative, so the result does not depend on
 // the order that atomics give terms inside a bucket.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
 #include <mutex>
 
 #include "launch.h"
@@ -30,6 +33,7 @@ namespace wbte {
 
 namespace {
 constexpr int TPB = 128;
+constexpr int SEG_TPB = 64;  // threads per block of k_segments
 inline unsigned blocks_for(int64_t n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
 
 template <class F> struct Aff;
@@ -231,7 +235,7 @@ void run_family(uint8_t* out, const uint8_t* points, const int64_t* pbase, const
     prof_begin(g1 ? "msm_segments_g1" : "msm_segments_g2", s, &tok);
     int64_t segthreads = k * p.windows * p.segments;
     note_launch();
-    k_segments<F><<<blocks_for(segthreads, 64), 64, 0, s>>>(seg, points, pbase, idx, entries, nnz, vsel, k, n,
+    k_segments<F><<<blocks_for(segthreads, SEG_TPB), SEG_TPB, 0, s>>>(seg, points, pbase, idx, entries, nnz, vsel, k, n,
                                                            p.windows, p.segment, p.segments);
     prof_end(tok, s);
     prof_begin(g1 ? "msm_reduce_g1" : "msm_reduce_g2", s, &tok);
@@ -256,7 +260,27 @@ void run_family(uint8_t* out, const uint8_t* points, const int64_t* pbase, const
 }
 }  // namespace
 
-MsmPlan msm_plan(int64_t n, int64_t k) {
+// Threads of k_segments<F> resident on the whole device (one wave), from the
+// occupancy of the compiled kernel; cached per device and group.
+static int64_t segment_wave_threads(Group g) {
+    static std::atomic<int64_t> cache[2][64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148 * 256;
+    int gi = g == GROUP_G1 ? 0 : 1;
+    int64_t v = cache[gi][dev].load();
+    if (v > 0) return v;
+    int sms = 0, blocks = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g == GROUP_G1)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_segments<Fp>, SEG_TPB, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_segments<Fp2>, SEG_TPB, 0);
+    v = (int64_t)(sms > 0 ? sms : 148) * (blocks > 0 ? blocks : 4) * SEG_TPB;
+    cache[gi][dev].store(v);
+    return v;
+}
+
+MsmPlan msm_plan(Group g, int64_t n, int64_t k) {
     MsmPlan p;
     int lg = 0;
     while ((int64_t(1) << (lg + 1)) <= n) lg++;
@@ -267,13 +291,30 @@ MsmPlan msm_plan(int64_t n, int64_t k) {
     p.c = c;
     p.windows = (256 + c - 1) / c;
     p.buckets = 1 << (c - 1);
-    // segment length: keep enough independent threads in flight
-    int64_t S = n;
-    int64_t want = 148 * 256;
-    while (S > 64 && k * p.windows * ((n + S - 1) / S) < want) S = (S + 1) / 2;
-    if (S < 1) S = 1;
-    p.segment = S;
-    p.segments = (n + S - 1) / S;
+    // Segments per (MSM, window): every thread of k_segments walks one
+    // segment, so the launch takes ceil(threads / wave) waves of the longest
+    // segment.  Cost model in mixed additions: S terms plus one full addition
+    // (~1.43 mixed additions) per bucket change, min(S, buckets), and the
+    // tree reduction of the segment sums.
+    const int64_t wave = segment_wave_threads(g);
+    const int64_t rows = k * p.windows;
+    const double nnz = (double)n * (1.0 - 1.0 / (double)(int64_t(1) << c));
+    double best = 1e300;
+    int64_t best_s = 1;
+    for (int64_t s = 1; s <= 1024 && s <= n; s++) {
+        double S = std::ceil(nnz / (double)s);
+        double per_thread = S + 1.43 * std::min(S, (double)p.buckets);
+        int64_t threads = rows * s;
+        double waves = std::ceil((double)threads / (double)wave);
+        double reduce = s > 1 ? 1.43 * 8.0 * std::ceil((double)threads / (8.0 * (double)wave)) : 0.0;
+        double cost = waves * per_thread + reduce;
+        if (cost < best * 0.999) {
+            best = cost;
+            best_s = s;
+        }
+    }
+    p.segment = (n + best_s - 1) / best_s;
+    p.segments = (n + p.segment - 1) / p.segment;
     if (p.segments < 1) p.segments = 1;
     return p;
 }
@@ -300,7 +341,7 @@ void launch_msm_family(Group g, uint8_t* out, const uint8_t* points, const int64
         cudaMemsetAsync(out, 0, (g == GROUP_G1 ? G1_AFF : G2_AFF) * (size_t)k, s);
         return;
     }
-    MsmPlan p = forced ? *forced : msm_plan(n, k);
+    MsmPlan p = forced ? *forced : msm_plan(g, n, k);
     size_t bytes = msm_family_scratch_bytes(g, V, k, n, p);
     void* scratch = nullptr;
     if (cudaMallocAsync(&scratch, bytes, s) != cudaSuccess) return;
@@ -364,7 +405,7 @@ extern "C" int32_t wbte_g1_msm_static(void* out, const void* points, const void*
         base = g_static_addr[dev];
     }
     if (n == 0) return cudaMemsetAsync(out, 0, G1_AFF, s) == cudaSuccess ? 0 : -5;
-    MsmPlan p = msm_plan((int64_t)n, 1);
+    MsmPlan p = msm_plan(GROUP_G1, (int64_t)n, 1);
     size_t need = msm_family_scratch_bytes(GROUP_G1, 1, 1, (int64_t)n, p);
     if (need > STATIC_MSM_BYTES - STATIC_MSM_TAIL) return -2;
     // point base of the single MSM: zero (the tail of the array is reused by

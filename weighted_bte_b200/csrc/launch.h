@@ -78,7 +78,7 @@ struct MsmPlan {
     int c = 0, windows = 0, buckets = 0;
     int64_t segment = 0, segments = 0;
 };
-MsmPlan msm_plan(int64_t n, int64_t k);
+MsmPlan msm_plan(Group g, int64_t n, int64_t k);
 void launch_msm_family(Group g, uint8_t* out, const uint8_t* points, const int64_t* pbase, const int32_t* idx,
                        const uint8_t* scalars, const int32_t* vsel, int32_t V, int64_t k, int64_t n,
                        cudaStream_t s, const MsmPlan* forced = nullptr);
