@@ -239,6 +239,39 @@ int32_t wbte_wbtx_keygen_material(wbte_ctx *ctx, const void *z, const int32_t *o
                                   const void *q_neg, uint64_t W, uint64_t N, uint64_t L,
                                   void *verification_keys, void *negative, void *positive);
 
+/* ------------------------------------------------------------- btx */
+/* MiddleProductKernel::new (btx/src/decryption.rs:131-190) for one batch size
+ * B <= L from the key powers low = [tau^1 .. tau^L] G2 and
+ * high = [tau^(L+2) .. tau^(2L)] G2:
+ *   kernel_lines   m * 68 * 288 bytes, m = next_pow2(2 B): lines of the
+ *                  transformed centered kernel scaled by 1/m
+ *   opening_lines  B * 68 * 288 bytes: lines of h_{-(slot+1)} = tau^(L-slot)
+ *   kernel         m G2 (the scaled transformed kernel), may be NULL. */
+int32_t wbte_btx_kernel(wbte_ctx *ctx, const void *low_powers, const void *high_powers, uint64_t L,
+                        uint64_t batch_size, void *kernel_lines, void *opening_lines, void *kernel);
+/* beta (precompute_batch, btx/src/decryption.rs:201-246): the middle product
+ * of wbte_wbtx_precompute over the btx kernel lines. */
+int32_t wbte_btx_precompute(wbte_ctx *ctx, void *beta, const void *kernel_lines, const void *first,
+                            const uint8_t *valid, uint64_t batch_size);
+/* sigma = sum_i shares[i] first[i] (partial_decrypt, btx/src/decryption.rs:248-264);
+ * first carries the identity at invalid slots. */
+int32_t wbte_btx_partial_decrypt(wbte_ctx *ctx, void *sigma, const void *first, const void *shares,
+                                 uint64_t batch_size);
+/* sigma = sum_j lambda_j sigmas[j] with the Lagrange coefficients at zero of
+ * the shares' domain points, in the given order (combine_shares,
+ * btx/src/decryption.rs:266-306). */
+int32_t wbte_btx_combine(wbte_ctx *ctx, void *sigma, const void *sigmas, const void *points, uint64_t T);
+/* *ok = 1 iff prod_{valid i} e(first_i, slot_points[i]) * e(-sigma, G2) == 1.
+ * slot_points = low powers: verify_combined_share (btx/src/decryption.rs:372-400);
+ * slot_points = one server's share commitments: verify_decryption_share (:340-370). */
+int32_t wbte_btx_verify(wbte_ctx *ctx, int32_t *ok, const void *first, const uint8_t *valid,
+                        uint64_t batch_size, const void *slot_points, uint64_t n_slot_points,
+                        const void *sigma);
+/* messages[i] = second[i] - e(sigma, h_{-(i+1)}) + beta[i] for valid slots
+ * (open_batch, btx/src/decryption.rs:402-458); invalid slots get the identity. */
+int32_t wbte_btx_open(wbte_ctx *ctx, void *messages, const void *opening_lines, const void *sigma,
+                      const void *second, const void *beta, const uint8_t *valid, uint64_t batch_size);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,6 +93,12 @@ _SIGNATURES = {
     "wbte_wbtx_open": [_VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64],
     "wbte_wbtx_keygen_material": [_VP, _VP, _VP, _VP, _U64, _U64, _U64, _VP, _VP, _VP],
     "wbte_measure_imad_rate": [_VP],
+    "wbte_btx_kernel": [_VP, _VP, _U64, _U64, _VP, _VP, _VP],
+    "wbte_btx_precompute": [_VP, _VP, _VP, _VP, _U64],
+    "wbte_btx_partial_decrypt": [_VP, _VP, _VP, _U64],
+    "wbte_btx_combine": [_VP, _VP, _VP, _U64],
+    "wbte_btx_verify": [_VP, _VP, _VP, _U64, _VP, _U64, _VP],
+    "wbte_btx_open": [_VP, _VP, _VP, _VP, _VP, _VP, _U64],
 }
 EXPORTED = sorted(
     list(_SIGNATURES)

@@ -899,4 +899,152 @@ int32_t wbte_wbtx_keygen_material(wbte_ctx* ctx, const void* z, const int32_t* o
     return c.finish();
 }
 
+// ------------------------------------------------------------------ btx
+int32_t wbte_btx_kernel(wbte_ctx* ctx, const void* low_powers, const void* high_powers, uint64_t L, uint64_t B,
+                        void* kernel_lines, void* opening_lines, void* kernel) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!low_powers || (L > 1 && !high_powers) || !kernel_lines || !opening_lines)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    if (B == 0 || B > L) return c.fail(WBTE_ERR_SIZE, "batch size out of range");
+    const uint64_t m = next_pow2(2 * B);
+    const int lgm = log2_exact(m);
+    uint8_t* dlines = c.out(kernel_lines, LINE_SZ * LINES_PER_POINT * m);
+    uint8_t* dopen = c.out(opening_lines, LINE_SZ * LINES_PER_POINT * B);
+    uint8_t* dkern_out = kernel ? c.out(kernel, G2_AFF * m) : nullptr;
+    const uint8_t* dlow = c.in(low_powers, G2_AFF * L);
+    const uint8_t* dhigh = L > 1 ? c.in(high_powers, G2_AFF * (L - 1)) : nullptr;
+    // centered powers h_e = power(L + 1 + e): h_{-d} = low[L - d], h_d = high[d - 1]
+    std::vector<int32_t> neg_idx, pos_idx, open_idx(B);
+    for (uint64_t d = 1; d < B; d++) neg_idx.push_back((int32_t)(L - d));
+    for (int64_t d = (int64_t)B - 1; d >= 1; d--) pos_idx.push_back((int32_t)(d - 1));
+    for (uint64_t slot = 0; slot < B; slot++) open_idx[slot] = (int32_t)(L - 1 - slot);  // h_{-(slot+1)}
+    std::vector<uint8_t> ones(FR_SZ * m, 0);
+    for (uint64_t i = 0; i < m; i++) ones[FR_SZ * i] = 1;
+    uint8_t* kern = c.zeros(G2_AFF * m);
+    uint8_t* work = c.alloc(G2_XYZZ * m);
+    uint8_t* opening = c.alloc(G2_AFF * B);
+    uint8_t* inv = const_cast<uint8_t*>(c.in_vec(ones));
+    const int32_t* dneg = B > 1 ? c.in_vec(neg_idx) : nullptr;
+    const int32_t* dpos = B > 1 ? c.in_vec(pos_idx) : nullptr;
+    const int32_t* dopi = c.in_vec(open_idx);
+    const uint8_t* tw = twiddles(c, (int64_t)m, false);
+    if (!c.ok()) return c.finish();
+    // K[0] = 0, K[d] = h_{-d}, K[m - d] = h_d (btx/src/decryption.rs:145-153)
+    if (B > 1) {
+        launch_gather(kern + G2_AFF, dlow, dneg, (int64_t)B - 1, G2_AFF, c.s);
+        launch_gather(kern + G2_AFF * (m - B + 1), dhigh, dpos, (int64_t)B - 1, G2_AFF, c.s);
+    }
+    launch_group_ntt(GROUP_G2, kern, work, tw, (int64_t)m, c.s);
+    // the inverse-transform factor 1/m moves into the kernel (:155-161)
+    launch_fr_scale_size_inv(inv, inv, lgm, (int64_t)m, c.s);
+    launch_mul_batch(GROUP_G2, kern, kern, 1, inv, (int64_t)m, c.s);
+    launch_prepare_lines(dlines, kern, (int64_t)m, c.s);
+    if (dkern_out) cudaMemcpyAsync(dkern_out, kern, G2_AFF * m, cudaMemcpyDeviceToDevice, c.s);
+    launch_gather(opening, dlow, dopi, (int64_t)B, G2_AFF, c.s);
+    launch_prepare_lines(dopen, opening, (int64_t)B, c.s);
+    return c.finish();
+}
+
+int32_t wbte_btx_precompute(wbte_ctx* ctx, void* beta, const void* kernel_lines, const void* first, const uint8_t* valid,
+                            uint64_t B) {
+    // the same middle product as weighted_btx (btx/src/decryption.rs:201-246)
+    return wbte_wbtx_precompute(ctx, beta, kernel_lines, first, valid, B);
+}
+
+int32_t wbte_btx_partial_decrypt(wbte_ctx* ctx, void* sigma, const void* first, const void* shares, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    if (B == 0) {
+        Call c(ctx);
+        return c.fail(WBTE_ERR_INVALID_ARG, "empty batch");
+    }
+    // sigma_j = sum_i share_{j,i} first_i (btx/src/decryption.rs:248-264)
+    return wbte_g1_msm(ctx, sigma, first, shares, B);
+}
+
+int32_t wbte_btx_combine(wbte_ctx* ctx, void* sigma, const void* sigmas, const void* points, uint64_t T) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!sigma || !sigmas || !points || T == 0) return c.fail(WBTE_ERR_INVALID_ARG, "null argument or no shares");
+    uint8_t* dsig = c.out(sigma, G1_AFF);
+    const uint8_t* ds = c.in(sigmas, G1_AFF * T);
+    const uint8_t* dx = c.in(points, FR_SZ * T);
+    uint8_t* lam = c.alloc(FR_SZ * T);
+    int32_t* status = (int32_t*)c.zeros(sizeof(int32_t));
+    std::vector<int64_t> zero(1, 0);
+    const int64_t* dzero = c.in_vec(zero);
+    if (!c.ok()) return c.finish();
+    launch_lagrange_at_zero(lam, dx, (int64_t)T, status, c.s);
+    launch_msm_family(GROUP_G1, dsig, ds, dzero, nullptr, lam, nullptr, 1, 1, (int64_t)T, c.s);
+    int32_t st = 0;
+    if (c.to_host(&st, status, sizeof(st)) && st) c.fail(WBTE_ERR_INTERPOLATION, "the interpolation points must be nonempty and distinct");
+    return c.finish();
+}
+
+int32_t wbte_btx_verify(wbte_ctx* ctx, int32_t* ok, const void* first, const uint8_t* valid, uint64_t B,
+                        const void* slot_points, uint64_t n_slot_points, const void* sigma) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!ok) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    *ok = 0;
+    if (!first || !valid || !slot_points || !sigma || B == 0) return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    if (n_slot_points < B) return c.fail(WBTE_ERR_SIZE, "fewer slot points than slots");
+    std::vector<uint8_t> hvalid(B);
+    if (!c.to_host(hvalid.data(), valid, B)) return c.finish();
+    std::vector<int32_t> slots;
+    for (uint64_t i = 0; i < B; i++)
+        if (hvalid[i]) slots.push_back((int32_t)i);
+    const int64_t nv = (int64_t)slots.size();
+    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint8_t* dq = c.in(slot_points, G2_AFF * n_slot_points);
+    const uint8_t* dsig = c.in(sigma, G1_AFF);
+    uint8_t* P = c.alloc(G1_AFF * (nv + 1));
+    uint8_t* Q = c.alloc(G2_AFF * (nv + 1));
+    uint8_t* f = c.alloc(GT_SZ * (nv + 1));
+    uint8_t* prod = c.alloc(GT_SZ);
+    uint8_t* flag = c.alloc(1);
+    const int32_t* dslots = nv ? c.in_vec(slots) : nullptr;
+    uint8_t* g2 = g2_generator_dev(c);
+    if (!c.ok()) return c.finish();
+    // prod_{valid i} e(first_i, Q_i) * e(-sigma, G2) == 1 (btx/src/decryption.rs:340-400)
+    if (nv > 0) {
+        launch_gather(P, dfirst, dslots, nv, G1_AFF, c.s);
+        launch_gather(Q, dq, dslots, nv, G2_AFF, c.s);
+    }
+    launch_negate(GROUP_G1, P + G1_AFF * nv, dsig, 1, c.s);
+    cudaMemcpyAsync(Q + G2_AFF * nv, g2, G2_AFF, cudaMemcpyDeviceToDevice, c.s);
+    launch_miller(f, P, Q, nv + 1, c.s);
+    fp12_product(c, prod, f, nv + 1);
+    launch_final_exp(prod, prod, 1, FE_FULL, c.s);
+    launch_fp12_is_one(flag, prod, 1, c.s);
+    uint8_t h = 0;
+    if (c.to_host(&h, flag, 1)) *ok = h ? 1 : 0;
+    return c.finish();
+}
+
+int32_t wbte_btx_open(wbte_ctx* ctx, void* messages, const void* opening_lines, const void* sigma, const void* second,
+                      const void* beta, const uint8_t* valid, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!messages || !opening_lines || !sigma || !second || !beta || !valid || B == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    uint8_t* dm = c.out(messages, GT_SZ * B);
+    const uint8_t* dl = c.in(opening_lines, LINE_SZ * LINES_PER_POINT * B);
+    const uint8_t* dsig = c.in(sigma, G1_AFF);
+    const uint8_t* d2 = c.in(second, GT_SZ * B);
+    const uint8_t* db = c.in(beta, GT_SZ * B);
+    const uint8_t* dv = c.in(valid, B);
+    uint8_t* P = c.alloc(G1_AFF * B);
+    uint8_t* alpha = c.alloc(GT_SZ * B);
+    std::vector<int32_t> zero_idx(B, 0);
+    const int32_t* dz = c.in_vec(zero_idx);
+    if (!c.ok()) return c.finish();
+    // alpha_slot = e(sigma, h_{-(slot+1)}) (btx/src/decryption.rs:402-458)
+    launch_gather(P, dsig, dz, (int64_t)B, G1_AFF, c.s);
+    launch_miller_lines(alpha, dl, P, (int64_t)B, c.s);
+    launch_final_exp(alpha, alpha, (int64_t)B, FE_FULL, c.s);
+    launch_unmask(dm, d2, alpha, db, dv, (int64_t)B, c.s);
+    return c.finish();
+}
+
 }  // extern "C"
