@@ -272,6 +272,65 @@ int32_t wbte_btx_verify(wbte_ctx *ctx, int32_t *ok, const void *first, const uin
 int32_t wbte_btx_open(wbte_ctx *ctx, void *messages, const void *opening_lines, const void *sigma,
                       const void *second, const void *beta, const uint8_t *valid, uint64_t batch_size);
 
+/* ---------------------------------------------------- weighted_pfe */
+typedef struct {
+    const void *domain_points;     /* total_weight Fr: the virtual points             */
+    const void *verification_keys; /* batch_size * party_count G2, slot-major: i N + j */
+    const void *d1;                /* batch_size * total_weight G2, slot-major         */
+    const void *d2;                /* batch_size * total_weight G2, slot-major         */
+    const void *global_key;        /* 1 G2: [z (beta_{-1} + beta_0)] G2                 */
+    const int64_t *party_offsets;  /* host, party_count + 1 prefix offsets              */
+    uint64_t party_count;
+    uint64_t total_weight;
+    uint64_t batch_size;           /* a power of two                                    */
+} wbte_wpfe_key;
+
+/* Party fractions g = 1 / (rho_j + alpha_i) and, when u is not NULL, the mask
+ * values u = g^2 + beta_{-1} / (alpha_i + 1) + beta_0 / alpha_i with
+ * masks = (beta_{-1}, beta_0) (weighted_pfe/src/setup.rs:223-247, :620-631);
+ * stored slot-major (i N + j) or party-major (j B + i). */
+int32_t wbte_wpfe_fractions(wbte_ctx *ctx, void *g, void *u, const void *rho, const void *alpha,
+                            const void *masks, uint64_t N, uint64_t B, int32_t party_major);
+/* Public key material (weighted_pfe/src/setup.rs:249-281) from slot-major g, u:
+ *   vk[i N + j] = [g_{j,i}] G2, d1[i W + w] = [z[w] g_{owner(w),i}] G2,
+ *   d2[i W + w] = [z[w] u_{owner(w),i}] G2.  owner host (W entries). */
+int32_t wbte_wpfe_keygen_material(wbte_ctx *ctx, const void *z, const int32_t *owner, const void *g,
+                                  const void *u, uint64_t W, uint64_t N, uint64_t B, void *vk, void *d1,
+                                  void *d2);
+/* sigma[j] = sum_i g_{j,i} first[i] for the T party secrets rho
+ * (partial_decrypt, weighted_pfe/src/decryption.rs:231-252). */
+int32_t wbte_wpfe_partial_decrypt(wbte_ctx *ctx, void *sigma, const void *first, const void *rho,
+                                  const void *alpha, uint64_t T, uint64_t B);
+/* *ok = 1 iff the random-linear aggregate share check passes
+ * (verify_decryption_shares_batched, weighted_pfe/src/decryption.rs:367-419);
+ * one share with challenge 1 is verify_decryption_share (:254-275). */
+int32_t wbte_wpfe_verify_shares(wbte_ctx *ctx, int32_t *ok, const wbte_wpfe_key *key, const void *first,
+                                const void *sigma, const int64_t *party_indices, const void *challenges,
+                                uint64_t T);
+/* Committee preparation (prepare_decryption, weighted_pfe/src/decryption.rs:421-538)
+ * for the accepted parties (host, ascending); mask_scalars = alpha_i (alpha_i + 1)
+ * for every slot, then -alpha_i for every slot (2 B Fr):
+ *   by_party     B * T G2: sum_{w in party k} lambda_w / 2B d1[i W + w]
+ *   total_lines  B line tables of sum_k by_party[i T + k]
+ *   mask_lines   B line tables of alpha(alpha+1) sum_w lambda_w d2[i W + w] - alpha V
+ *   total, mask  B G2 each, may be NULL. */
+int32_t wbte_wpfe_prepare(wbte_ctx *ctx, const wbte_wpfe_key *key, const int64_t *party_indices, uint64_t T,
+                          const void *mask_scalars, void *by_party, void *total_lines, void *mask_lines,
+                          void *total, void *mask);
+/* Cauchy sums (precompute_batch, weighted_pfe/src/decryption.rs:540-574, :683-734):
+ *   first_cauchy[i]   = 2B sum_{k != i} first[k] / (alpha_k - alpha_i)
+ *   pairing_cauchy[i] = the same sums over e(first[k], total_k) on easy-final-
+ *                       exponentiated values (canonical after the hard part). */
+int32_t wbte_wpfe_precompute(wbte_ctx *ctx, void *first_cauchy, void *pairing_cauchy, const void *first,
+                             const void *total_lines, uint64_t B);
+/* messages[i] = second[i] - hard(e(first_i, mask_i) / (prod_k e(2B sigma_k -
+ * first_cauchy[i], by_party[i T + k]) pairing_cauchy[i])^(alpha_i (alpha_i + 1)))
+ * (open_batch, weighted_pfe/src/decryption.rs:576-644); alpha_products B Fr. */
+int32_t wbte_wpfe_open(wbte_ctx *ctx, void *messages, const void *sigmas, uint64_t T, const void *by_party,
+                       const void *first, const void *mask_lines, const void *first_cauchy,
+                       const void *pairing_cauchy, const void *second, const void *alpha_products,
+                       uint64_t B);
+
 #ifdef __cplusplus
 }
 #endif

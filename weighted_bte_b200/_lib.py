@@ -57,6 +57,20 @@ class WbtxKey(ctypes.Structure):
     ]
 
 
+class WpfeKey(ctypes.Structure):
+    _fields_ = [
+        ("domain_points", ctypes.c_void_p),
+        ("verification_keys", ctypes.c_void_p),
+        ("d1", ctypes.c_void_p),
+        ("d2", ctypes.c_void_p),
+        ("global_key", ctypes.c_void_p),
+        ("party_offsets", ctypes.c_void_p),
+        ("party_count", ctypes.c_uint64),
+        ("total_weight", ctypes.c_uint64),
+        ("batch_size", ctypes.c_uint64),
+    ]
+
+
 _VP, _U64, _I32, _I64 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int64
 # name -> argument types after the context pointer
 _SIGNATURES = {
@@ -99,6 +113,13 @@ _SIGNATURES = {
     "wbte_btx_combine": [_VP, _VP, _VP, _U64],
     "wbte_btx_verify": [_VP, _VP, _VP, _U64, _VP, _U64, _VP],
     "wbte_btx_open": [_VP, _VP, _VP, _VP, _VP, _VP, _U64],
+    "wbte_wpfe_fractions": [_VP, _VP, _VP, _VP, _VP, _U64, _U64, _I32],
+    "wbte_wpfe_keygen_material": [_VP, _VP, _VP, _VP, _U64, _U64, _U64, _VP, _VP, _VP],
+    "wbte_wpfe_partial_decrypt": [_VP, _VP, _VP, _VP, _U64, _U64],
+    "wbte_wpfe_verify_shares": [_VP, _VP, _VP, _VP, _VP, _VP, _U64],
+    "wbte_wpfe_prepare": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP],
+    "wbte_wpfe_precompute": [_VP, _VP, _VP, _VP, _U64],
+    "wbte_wpfe_open": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64],
 }
 EXPORTED = sorted(
     list(_SIGNATURES)

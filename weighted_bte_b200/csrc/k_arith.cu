@@ -70,6 +70,27 @@ __global__ void k_material_scalars(uint8_t* out, const uint8_t* z, const int32_t
     store_fr_canonical(out + FR_SZ * i, fr_mul(x, y));
 }
 
+// Partial-fraction party keys of weighted_pfe (setup.rs:223-247):
+//   g = 1 / (rho_j + alpha_i),  u = g^2 + beta_{-1} / (alpha_i + 1) + beta_0 / alpha_i
+// stored at i * N + j (slot-major) or j * B + i (party-major); u may be null.
+__global__ void k_wpfe_fractions(uint8_t* g, uint8_t* u, const uint8_t* rho, const uint8_t* alpha,
+                                 const uint8_t* masks, int64_t N, int64_t B, int party_major) {
+    int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (x >= N * B) return;
+    int64_t i = x / N, j = x % N;
+    int64_t o = party_major ? j * B + i : x;
+    Fr a = load_fr_mont(alpha + FR_SZ * i);
+    Fr gi = fr_inv(fr_add(load_fr_mont(rho + FR_SZ * j), a));
+    store_fr_canonical(g + FR_SZ * o, gi);
+    if (u) {
+        Fr bm1 = load_fr_mont(masks), b0 = load_fr_mont(masks + FR_SZ);
+        Fr t = fr_mul(gi, gi);
+        t = fr_add(t, fr_mul(bm1, fr_inv(fr_add(a, fr_one()))));
+        t = fr_add(t, fr_mul(b0, fr_inv(a)));
+        store_fr_canonical(u + FR_SZ * o, t);
+    }
+}
+
 __global__ void k_gather(uint8_t* out, const uint8_t* in, const int32_t* idx, int64_t n, int64_t record) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -393,6 +414,13 @@ void launch_material_scalars(uint8_t* out, const uint8_t* z, const int32_t* owne
     if (rows * W <= 0) return;
     note_launch();
     k_material_scalars<<<blocks_for(rows * W), TPB, 0, s>>>(out, z, owner, qp, W, N, rows);
+}
+void launch_wpfe_fractions(uint8_t* g, uint8_t* u, const uint8_t* rho, const uint8_t* alpha, const uint8_t* masks,
+                           int64_t N, int64_t B, bool party_major, cudaStream_t s) {
+    ProfScope prof_("fr_fractions", s);
+    if (N * B <= 0) return;
+    note_launch();
+    k_wpfe_fractions<<<blocks_for(N * B), TPB, 0, s>>>(g, u, rho, alpha, masks, N, B, party_major ? 1 : 0);
 }
 void launch_gather(uint8_t* out, const uint8_t* in, const int32_t* idx, int64_t n, int64_t record, cudaStream_t s) {
     if (n <= 0) return;

@@ -235,6 +235,14 @@ __global__ void k_gt_compress(uint8_t* out, const uint8_t* in, int64_t n) {
     }
 }
 
+__global__ void k_fp12_conj(uint8_t* out, const uint8_t* in, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fp12 x = load_vec(as_gt(in) + i);
+    fp12_conj(x, x);
+    store_vec(as_gt(out) + i, x);
+}
+
 __global__ void k_fp12_mask(uint8_t* io, const uint8_t* valid, int64_t n) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -334,6 +342,11 @@ void launch_gt_compress(uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t
     if (n <= 0) return;
     note_launch();
     k_gt_compress<<<blocks_for(n), TPB, 0, s>>>(out, in, n);
+}
+void launch_fp12_conj(uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    note_launch();
+    k_fp12_conj<<<blocks_for(n), TPB, 0, s>>>(out, in, n);
 }
 void launch_fp12_is_one(uint8_t* flags, const uint8_t* in, int64_t n, cudaStream_t s) {
     if (n <= 0) return;

@@ -47,6 +47,10 @@ void launch_material_scalars(uint8_t* out, const uint8_t* z, const int32_t* owne
                              int64_t N, int64_t rows, cudaStream_t s);
 // out[i] = in[idx[i]] for fixed-size records
 void launch_gather(uint8_t* out, const uint8_t* in, const int32_t* idx, int64_t n, int64_t record, cudaStream_t s);
+// weighted_pfe party fractions g = 1/(rho_j + alpha_i) and mask values u
+// (u may be null); slot-major (i * N + j) or party-major (j * B + i).
+void launch_wpfe_fractions(uint8_t* g, uint8_t* u, const uint8_t* rho, const uint8_t* alpha, const uint8_t* masks,
+                           int64_t N, int64_t B, bool party_major, cudaStream_t s);
 // Lagrange coefficients at zero of the points x[0..n) (direct formula); status[0] = 1 on a repeated point
 void launch_lagrange_at_zero(uint8_t* out, const uint8_t* x, int64_t n, int32_t* status, cudaStream_t s);
 // tw[j] = w^j, j < count, w = generator (or its inverse) of the size-n domain; canonical
@@ -109,6 +113,8 @@ void launch_gt_ntt(uint8_t* io, const uint8_t* twiddles, int64_t n, cudaStream_t
 void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t base_stride, const uint8_t* scalars, int64_t n, cudaStream_t s);
 // out[i] = a[i * sa] * b[i * sb] (conj_b: b conjugated)
 void launch_fp12_mul(uint8_t* out, const uint8_t* a, int64_t sa, const uint8_t* b, int64_t sb, bool conj_b, int64_t n, cudaStream_t s);
+// out[i] = conjugate of in[i] (the inverse in the cyclotomic subgroup)
+void launch_fp12_conj(uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
 // messages[i] = valid[i] ? second[i] * conj(alpha[i]) * beta[i] : one
 void launch_unmask(uint8_t* out, const uint8_t* second, const uint8_t* alpha, const uint8_t* beta, const uint8_t* valid, int64_t n, cudaStream_t s);
 // torus-compressed GT encodings (tag byte + 288 bytes)

@@ -1047,4 +1047,326 @@ int32_t wbte_btx_open(wbte_ctx* ctx, void* messages, const void* opening_lines, 
     return c.finish();
 }
 
+// ---------------------------------------------------------- weighted_pfe
+// canonical little-endian encoding of a small signed integer modulo r
+static std::vector<uint8_t> fr_small_signed(const std::vector<int64_t>& c) {
+    static const uint64_t R_LIMBS[4] = {0xffffffff00000001ull, 0x53bda402fffe5bfeull, 0x3339d80809a1d805ull,
+                                        0x73eda753299d7d48ull};
+    std::vector<uint8_t> out(FR_SZ * c.size(), 0);
+    for (size_t i = 0; i < c.size(); i++) {
+        uint64_t v[4] = {0, 0, 0, 0};
+        if (c[i] >= 0) {
+            v[0] = (uint64_t)c[i];
+        } else {
+            uint64_t mag = (uint64_t)(-(c[i] + 1)) + 1, borrow = 0;
+            for (int k = 0; k < 4; k++) {
+                uint64_t sub = (k == 0 ? mag : 0) + borrow;
+                uint64_t nb = (R_LIMBS[k] < sub || (sub == 0 && borrow)) ? 1 : 0;
+                v[k] = R_LIMBS[k] - sub;
+                borrow = nb;
+            }
+        }
+        memcpy(out.data() + FR_SZ * i, v, FR_SZ);
+    }
+    return out;
+}
+
+static int32_t check_wpfe_key(Call& c, const wbte_wpfe_key* key) {
+    if (!key || !key->party_offsets || key->party_count == 0 || key->batch_size == 0 || key->total_weight == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "invalid weighted-PFE key");
+    if ((uint64_t)key->party_offsets[key->party_count] != key->total_weight)
+        return c.fail(WBTE_ERR_INVALID_ARG, "party offsets do not sum to the total weight");
+    if (log2_exact(key->batch_size) < 0) return c.fail(WBTE_ERR_SIZE, "batch size must be a power of two");
+    return WBTE_OK;
+}
+
+int32_t wbte_wpfe_fractions(wbte_ctx* ctx, void* g, void* u, const void* rho, const void* alpha, const void* masks,
+                            uint64_t N, uint64_t B, int32_t party_major) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!g || !rho || !alpha || (u && !masks) || N == 0 || B == 0) return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty dimension");
+    uint8_t* dg = c.out(g, FR_SZ * N * B);
+    uint8_t* du = u ? c.out(u, FR_SZ * N * B) : nullptr;
+    const uint8_t* dr = c.in(rho, FR_SZ * N);
+    const uint8_t* da = c.in(alpha, FR_SZ * B);
+    const uint8_t* dm = u ? c.in(masks, 2 * FR_SZ) : nullptr;
+    if (c.ok()) launch_wpfe_fractions(dg, du, dr, da, dm, (int64_t)N, (int64_t)B, party_major != 0, c.s);
+    return c.finish();
+}
+
+int32_t wbte_wpfe_keygen_material(wbte_ctx* ctx, const void* z, const int32_t* owner, const void* g, const void* u,
+                                  uint64_t W, uint64_t N, uint64_t B, void* vk, void* d1, void* d2) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!z || !owner || !g || !u || !vk || !d1 || !d2 || W == 0 || N == 0 || B == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty dimension");
+    for (uint64_t w = 0; w < W; w++)
+        if (owner[w] < 0 || (uint64_t)owner[w] >= N) return c.fail(WBTE_ERR_INVALID_ARG, "owner index out of range");
+    uint8_t* dvk = c.out(vk, G2_AFF * B * N);
+    uint8_t* dd1 = c.out(d1, G2_AFF * B * W);
+    uint8_t* dd2 = c.out(d2, G2_AFF * B * W);
+    const uint8_t* dz = c.in(z, FR_SZ * W);
+    const uint8_t* dg = c.in(g, FR_SZ * B * N);
+    const uint8_t* du = c.in(u, FR_SZ * B * N);
+    std::vector<int32_t> ho(owner, owner + W);
+    const int32_t* downer = c.in_vec(ho);
+    const uint64_t rows_per_chunk = std::max<uint64_t>(1, (uint64_t(1) << 20) / W);
+    uint8_t* sc = c.alloc(FR_SZ * W * std::min<uint64_t>(rows_per_chunk, B));
+    if (!c.ok()) return c.finish();
+    // vk[i N + j] = [g_{j,i}] G2; D[i W + w] = [Z(w) g_{owner(w),i}] G2; U likewise with u
+    launch_mul_generator(GROUP_G2, dvk, dg, (int64_t)(B * N), c.s);
+    for (int pass = 0; pass < 2; pass++) {
+        const uint8_t* q = pass == 0 ? dg : du;
+        uint8_t* dst = pass == 0 ? dd1 : dd2;
+        for (uint64_t r0 = 0; r0 < B; r0 += rows_per_chunk) {
+            uint64_t nr = std::min(rows_per_chunk, B - r0);
+            launch_material_scalars(sc, dz, downer, q + FR_SZ * r0 * N, (int64_t)W, (int64_t)N, (int64_t)nr, c.s);
+            launch_mul_generator(GROUP_G2, dst + G2_AFF * r0 * W, sc, (int64_t)(nr * W), c.s);
+        }
+    }
+    return c.finish();
+}
+
+int32_t wbte_wpfe_partial_decrypt(wbte_ctx* ctx, void* sigma, const void* first, const void* rho, const void* alpha,
+                                  uint64_t T, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (T == 0) return c.finish();
+    if (!sigma || !first || !rho || !alpha || B == 0) return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    uint8_t* dsig = c.out(sigma, G1_AFF * T);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint8_t* dr = c.in(rho, FR_SZ * T);
+    const uint8_t* da = c.in(alpha, FR_SZ * B);
+    uint8_t* g = c.alloc(FR_SZ * T * B);
+    std::vector<int64_t> base(T, 0);
+    std::vector<int32_t> vsel(T);
+    for (uint64_t j = 0; j < T; j++) vsel[j] = (int32_t)j;
+    const int64_t* db = c.in_vec(base);
+    const int32_t* dv = c.in_vec(vsel);
+    if (!c.ok()) return c.finish();
+    // sigma_j = sum_i g_{j,i} first_i (weighted_pfe/src/decryption.rs:231-252)
+    launch_wpfe_fractions(g, nullptr, dr, da, nullptr, (int64_t)T, (int64_t)B, true, c.s);
+    launch_msm_family(GROUP_G1, dsig, dfirst, db, nullptr, g, dv, (int32_t)T, (int64_t)T, (int64_t)B, c.s);
+    return c.finish();
+}
+
+int32_t wbte_wpfe_verify_shares(wbte_ctx* ctx, int32_t* ok, const wbte_wpfe_key* key, const void* first,
+                                const void* sigma, const int64_t* party_indices, const void* challenges, uint64_t T) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    {
+        Call c(ctx);
+        if (check_wpfe_key(c, key)) return c.finish();
+        if (!ok) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    }
+    // the weighted_btx aggregate check with every slot valid
+    // (weighted_pfe/src/decryption.rs:367-419 and :254-275)
+    wbte_wbtx_key wk;
+    wk.domain_points = key->domain_points;
+    wk.verification_keys = key->verification_keys;
+    wk.negative_material = key->d1;
+    wk.positive_material = key->d2;
+    wk.party_offsets = key->party_offsets;
+    wk.party_count = key->party_count;
+    wk.total_weight = key->total_weight;
+    wk.max_batch_size = key->batch_size;
+    std::vector<uint8_t> valid(key->batch_size, 1);
+    return wbte_wbtx_verify_shares(ctx, ok, &wk, first, valid.data(), key->batch_size, sigma, party_indices, challenges, T);
+}
+
+int32_t wbte_wpfe_prepare(wbte_ctx* ctx, const wbte_wpfe_key* key, const int64_t* party_indices, uint64_t T,
+                          const void* mask_scalars, void* by_party, void* total_lines, void* mask_lines, void* total,
+                          void* mask) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (check_wpfe_key(c, key)) return c.finish();
+    if (!party_indices || T == 0 || !mask_scalars || !by_party || !total_lines || !mask_lines || !key->d1 || !key->d2 ||
+        !key->global_key || !key->domain_points)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    const uint64_t N = key->party_count, W = key->total_weight, B = key->batch_size;
+    const int lg2b = log2_exact(2 * B);
+    std::vector<int32_t> sel;
+    std::vector<int64_t> coef_off(1, 0), party_base(T);
+    for (uint64_t k = 0; k < T; k++) {
+        int64_t j = party_indices[k];
+        if (j < 0 || (uint64_t)j >= N) return c.fail(WBTE_ERR_INVALID_ARG, "invalid party index");
+        if (k && party_indices[k - 1] >= j) return c.fail(WBTE_ERR_INVALID_ARG, "party indices must be strictly ascending");
+        for (int64_t w = key->party_offsets[j]; w < key->party_offsets[j + 1]; w++) sel.push_back((int32_t)w);
+        coef_off.push_back((int64_t)sel.size());
+        party_base[k] = key->party_offsets[j];
+    }
+    const int64_t WT = (int64_t)sel.size();
+    uint8_t* dby = c.out(by_party, G2_AFF * B * T);
+    uint8_t* dtl = c.out(total_lines, LINE_SZ * LINES_PER_POINT * B);
+    uint8_t* dml = c.out(mask_lines, LINE_SZ * LINES_PER_POINT * B);
+    uint8_t* dtot_out = total ? c.out(total, G2_AFF * B) : nullptr;
+    uint8_t* dmask_out = mask ? c.out(mask, G2_AFF * B) : nullptr;
+    const uint8_t* ddom = c.in(key->domain_points, FR_SZ * W);
+    const uint8_t* dd1 = c.in(key->d1, G2_AFF * B * W);
+    const uint8_t* dd2 = c.in(key->d2, G2_AFF * B * W);
+    const uint8_t* dV = c.in(key->global_key, G2_AFF);
+    const uint8_t* dms = c.in(mask_scalars, 2 * FR_SZ * B);
+    const int32_t* dsel = c.in_vec(sel);
+    uint8_t* x = c.alloc(FR_SZ * WT);
+    uint8_t* lam = c.alloc(FR_SZ * WT);
+    uint8_t* lam_s = c.alloc(FR_SZ * WT);
+    int32_t* status = (int32_t*)c.zeros(sizeof(int32_t));
+    uint8_t* tmp = c.alloc(G2_AFF * B);
+    uint8_t* tot = c.alloc(G2_AFF * B);
+    uint8_t* d2t = c.alloc(G2_AFF * B);
+    uint8_t* pairs = c.alloc(2 * G2_AFF * B);
+    uint8_t* msk = c.alloc(G2_AFF * B);
+    // segment offsets carry k + 1 entries for k segments
+    std::vector<int64_t> slot_base(B), offs_T(B + 1), offs_2(B + 1), d2base(B);
+    for (uint64_t i = 0; i <= B; i++) {
+        offs_T[i] = (int64_t)(i * T);
+        offs_2[i] = (int64_t)(2 * i);
+        if (i < B) d2base[i] = (int64_t)(i * W);
+    }
+    const int64_t* doffT = c.in_vec(offs_T);
+    const int64_t* doff2 = c.in_vec(offs_2);
+    const int64_t* dd2b = c.in_vec(d2base);
+    if (!c.ok()) return c.finish();
+    // Lagrange coefficients of the accepted virtual points; lambda / 2B for D
+    launch_gather(x, ddom, dsel, WT, FR_SZ, c.s);
+    launch_lagrange_at_zero(lam, x, WT, status, c.s);
+    launch_fr_scale_size_inv(lam_s, lam, lg2b, WT, c.s);
+    // scaled_d1_by_party[i T + k] = sum_{w in party k} lambda_w / 2B D[i W + w]
+    for (uint64_t k = 0; k < T; k++) {
+        for (uint64_t i = 0; i < B; i++) slot_base[i] = (int64_t)(i * W) + party_base[k];
+        const int64_t* dbase = c.in_vec(slot_base);
+        if (!c.ok()) return c.finish();
+        int64_t wk = coef_off[k + 1] - coef_off[k];
+        launch_msm_family(GROUP_G2, tmp, dd1, dbase, nullptr, lam_s + FR_SZ * coef_off[k], nullptr, 1, (int64_t)B, wk, c.s);
+        cudaMemcpy2DAsync(dby + G2_AFF * k, G2_AFF * T, tmp, G2_AFF, G2_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    }
+    launch_segment_sum(GROUP_G2, tot, dby, doffT, (int64_t)B, c.s);
+    // mask_i = alpha_i (alpha_i + 1) sum_w lambda_w U[i W + w] - alpha_i V
+    launch_msm_family(GROUP_G2, d2t, dd2, dd2b, dsel, lam, nullptr, 1, (int64_t)B, WT, c.s);
+    launch_mul_batch(GROUP_G2, tmp, d2t, 1, dms, (int64_t)B, c.s);
+    cudaMemcpy2DAsync(pairs, 2 * G2_AFF, tmp, G2_AFF, G2_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    launch_mul_batch(GROUP_G2, tmp, dV, 0, dms + FR_SZ * B, (int64_t)B, c.s);
+    cudaMemcpy2DAsync(pairs + G2_AFF, 2 * G2_AFF, tmp, G2_AFF, G2_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(GROUP_G2, msk, pairs, doff2, (int64_t)B, c.s);
+    launch_prepare_lines(dtl, tot, (int64_t)B, c.s);
+    launch_prepare_lines(dml, msk, (int64_t)B, c.s);
+    if (dtot_out) cudaMemcpyAsync(dtot_out, tot, G2_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    if (dmask_out) cudaMemcpyAsync(dmask_out, msk, G2_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    int32_t st = 0;
+    if (c.to_host(&st, status, sizeof(st)) && st) c.fail(WBTE_ERR_INTERPOLATION, "the interpolation points must be nonempty and distinct");
+    return c.finish();
+}
+
+int32_t wbte_wpfe_precompute(wbte_ctx* ctx, void* first_cauchy, void* pairing_cauchy, const void* first,
+                             const void* total_lines, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!first_cauchy || !pairing_cauchy || !first || !total_lines || B == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    if (log2_exact(B) < 0) return c.fail(WBTE_ERR_SIZE, "batch size must be a power of two");
+    uint8_t* dfc = c.out(first_cauchy, G1_AFF * B);
+    uint8_t* dpc = c.out(pairing_cauchy, GT_SZ * B);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint8_t* dl = c.in(total_lines, LINE_SZ * LINES_PER_POINT * B);
+    // closed-form Cauchy spectrum B - 1 - 2k (weighted_pfe/src/decryption.rs:194-213)
+    std::vector<int64_t> coeff(B);
+    std::vector<int32_t> rot(B);
+    for (uint64_t k = 0; k < B; k++) {
+        coeff[k] = (int64_t)B - 1 - 2 * (int64_t)k;
+        rot[k] = (int32_t)((k + B - 1) % B);
+    }
+    const uint8_t* dcoef = c.in_vec(fr_small_signed(coeff));
+    const int32_t* drot = c.in_vec(rot);
+    uint8_t* x = c.alloc(G1_AFF * B);
+    uint8_t* y = c.alloc(G1_AFF * B);
+    uint8_t* work = c.alloc(G1_XYZZ * B);
+    uint8_t* f = c.alloc(GT_SZ * B);
+    uint8_t* h = c.alloc(GT_SZ * B);
+    const uint8_t* tw = B > 1 ? twiddles(c, (int64_t)B, false) : nullptr;
+    const uint8_t* twi = B > 1 ? twiddles(c, (int64_t)B, true) : nullptr;
+    if (!c.ok()) return c.finish();
+    // G1: 2B sum_{k != i} first_k / (alpha_k - alpha_i) (:683-708)
+    cudaMemcpyAsync(x, dfirst, G1_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    if (B > 1) launch_group_ntt(GROUP_G1, x, work, tw, (int64_t)B, c.s);
+    launch_mul_batch(GROUP_G1, y, x, 1, dcoef, (int64_t)B, c.s);
+    launch_gather(x, y, drot, (int64_t)B, G1_AFF, c.s);
+    launch_negate(GROUP_G1, x, x, (int64_t)B, c.s);
+    if (B > 1) launch_group_ntt(GROUP_G1, x, work, twi, (int64_t)B, c.s);
+    cudaMemcpyAsync(dfc, x, G1_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    // GT: the same sums over e(first_k, D1_k) on easy-final-exponentiated values (:710-734)
+    launch_miller_lines(f, dl, dfirst, (int64_t)B, c.s);
+    launch_final_exp(f, f, (int64_t)B, FE_EASY, c.s);
+    if (B > 1) launch_gt_ntt(f, tw, (int64_t)B, c.s);
+    launch_gt_pow(h, f, 1, dcoef, (int64_t)B, c.s);
+    launch_gather(f, h, drot, (int64_t)B, GT_SZ, c.s);
+    launch_fp12_conj(f, f, (int64_t)B, c.s);
+    if (B > 1) launch_gt_ntt(f, twi, (int64_t)B, c.s);
+    cudaMemcpyAsync(dpc, f, GT_SZ * B, cudaMemcpyDeviceToDevice, c.s);
+    return c.finish();
+}
+
+int32_t wbte_wpfe_open(wbte_ctx* ctx, void* messages, const void* sigmas, uint64_t T, const void* by_party,
+                       const void* first, const void* mask_lines, const void* first_cauchy, const void* pairing_cauchy,
+                       const void* second, const void* alpha_products, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!messages || !sigmas || T == 0 || !by_party || !first || !mask_lines || !first_cauchy || !pairing_cauchy ||
+        !second || !alpha_products || B == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    uint8_t* dm = c.out(messages, GT_SZ * B);
+    const uint8_t* ds = c.in(sigmas, G1_AFF * T);
+    const uint8_t* dby = c.in(by_party, G2_AFF * B * T);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint8_t* dml = c.in(mask_lines, LINE_SZ * LINES_PER_POINT * B);
+    const uint8_t* dfc = c.in(first_cauchy, G1_AFF * B);
+    const uint8_t* dpc = c.in(pairing_cauchy, GT_SZ * B);
+    const uint8_t* d2 = c.in(second, GT_SZ * B);
+    const uint8_t* dap = c.in(alpha_products, FR_SZ * B);
+    const uint8_t* d2b = c.in_vec(fr_small_signed(std::vector<int64_t>(T, 2 * (int64_t)B)));
+    std::vector<int32_t> idx_share(B * T), idx_slot(B * T);
+    // segment offsets carry k + 1 entries for k segments
+    std::vector<int64_t> offs_T(B + 1), offs_2(B * T + 1);
+    for (uint64_t i = 0; i < B; i++)
+        for (uint64_t k = 0; k < T; k++) {
+            idx_share[i * T + k] = (int32_t)k;
+            idx_slot[i * T + k] = (int32_t)i;
+        }
+    for (uint64_t x = 0; x <= B * T; x++) offs_2[x] = (int64_t)(2 * x);
+    for (uint64_t i = 0; i <= B; i++) offs_T[i] = (int64_t)(i * T);
+    const int32_t* dis = c.in_vec(idx_share);
+    const int32_t* dil = c.in_vec(idx_slot);
+    const int64_t* doT = c.in_vec(offs_T);
+    const int64_t* do2 = c.in_vec(offs_2);
+    uint8_t* scaled = c.alloc(G1_AFF * T);
+    uint8_t* negfc = c.alloc(G1_AFF * B);
+    uint8_t* g0 = c.alloc(G1_AFF * B * T);
+    uint8_t* g1 = c.alloc(G1_AFF * B * T);
+    uint8_t* pairs = c.alloc(2 * G1_AFF * B * T);
+    uint8_t* left = c.alloc(G1_AFF * B * T);
+    uint8_t* f = c.alloc(GT_SZ * B * T);
+    uint8_t* ft = c.alloc(GT_SZ * B);
+    uint8_t* mp = c.alloc(GT_SZ * B);
+    if (!c.ok()) return c.finish();
+    // left[i T + k] = 2B sigma_k - scaled_first_cauchy[i] (weighted_pfe/src/decryption.rs:596-612)
+    launch_mul_batch(GROUP_G1, scaled, ds, 1, d2b, (int64_t)T, c.s);
+    launch_negate(GROUP_G1, negfc, dfc, (int64_t)B, c.s);
+    launch_gather(g0, scaled, dis, (int64_t)(B * T), G1_AFF, c.s);
+    launch_gather(g1, negfc, dil, (int64_t)(B * T), G1_AFF, c.s);
+    cudaMemcpy2DAsync(pairs, 2 * G1_AFF, g0, G1_AFF, G1_AFF, B * T, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(pairs + G1_AFF, 2 * G1_AFF, g1, G1_AFF, G1_AFF, B * T, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(GROUP_G1, left, pairs, do2, (int64_t)(B * T), c.s);
+    // first terms: per-slot multi-Miller loops over the T parties; mask pairings
+    launch_miller(f, left, dby, (int64_t)(B * T), c.s);
+    launch_fp12_segment_product(ft, f, doT, (int64_t)B, c.s);
+    launch_miller_lines(mp, dml, dfirst, (int64_t)B, c.s);
+    launch_final_exp(ft, ft, (int64_t)B, FE_EASY, c.s);
+    launch_final_exp(mp, mp, (int64_t)B, FE_EASY, c.s);
+    // mask = hard(mp / (ft pairing_cauchy)^(alpha (alpha + 1))); message = second / mask (:614-643)
+    launch_fp12_mul(ft, ft, 1, dpc, 1, false, (int64_t)B, c.s);
+    launch_gt_pow(f, ft, 1, dap, (int64_t)B, c.s);
+    launch_fp12_mul(mp, mp, 1, f, 1, true, (int64_t)B, c.s);
+    launch_final_exp(mp, mp, (int64_t)B, FE_HARD, c.s);
+    launch_fp12_mul(dm, d2, 1, mp, 1, true, (int64_t)B, c.s);
+    return c.finish();
+}
+
 }  // extern "C"

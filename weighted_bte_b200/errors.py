@@ -1,4 +1,5 @@
-"""Error contract of the weighted-BTX API (weighted_btx/src/error.rs:4-52).
+"""Error contract of the weighted-BTX and weighted-PFE APIs (weighted_btx/src/error.rs:4-52;
+weighted_pfe/src/error.rs:3-46 adds InvalidSecretKey and InvalidProof).
 
 Every variant of the reference's `Error` enum is one exception class with
 the same fields; all derive from `Error`.  Messages follow the reference's
@@ -127,3 +128,13 @@ class MismatchedSetup(Error):
 class MismatchedCommittee(Error):
     def __init__(self):
         super().__init__("decryption material belongs to a different accepted committee")
+
+
+class InvalidSecretKey(Error):
+    def __init__(self):
+        super().__init__("the party secret key produces a zero partial-fraction denominator")
+
+
+class InvalidProof(Error):
+    def __init__(self):
+        super().__init__("the ciphertext batch contains an invalid proof")
