@@ -331,6 +331,30 @@ int32_t wbte_wpfe_open(wbte_ctx *ctx, void *messages, const void *sigmas, uint64
                        const void *pairing_cauchy, const void *second, const void *alpha_products,
                        uint64_t B);
 
+/* ------------------------------------------------------------- pfe */
+/* PartialFractionKernel::new (pfe/src/decryption.rs:151-257) from the slot
+ * fraction keys DK_i = [1/(x + w^i)] G2 (B, a power of two) and their sum.
+ * scalars: 6 B Fr, in blocks of B: 1/(2B) | B-1-2k mod r | c (gamma = 1/c) |
+ * s2_i = w^i c | -s2_i | -(2B s1_i) o_i with s1_i = w^i (s2_i - 1) and o_i the
+ * opening coefficient w^-i (B+1)/2 + 1/(w^i - gamma).  Outputs line tables of
+ * DK_i/(2B), [s2_i] G2 and the fused third operand; the affine points
+ * (scaled_keys, generators, mixes, B G2 each) may be NULL. */
+int32_t wbte_pfe_kernel(wbte_ctx *ctx, const void *fraction_keys, const void *key_sum, uint64_t B,
+                        const void *scalars, void *key_lines, void *generator_lines, void *mix_lines,
+                        void *scaled_keys, void *generators, void *mixes);
+/* precompute_batch (pfe/src/decryption.rs:259-298): the gamma-weighted cyclic
+ * convolutions of first and of e(first_i, DK_i/(2B)); scalars: 2 B Fr
+ * (B-1-2k mod r | c). */
+int32_t wbte_pfe_precompute(wbte_ctx *ctx, void *weighted_first, void *weighted_pairings, const void *first,
+                            const void *key_lines, const void *scalars, uint64_t B);
+/* open_batch (pfe/src/decryption.rs:417-469): messages[i] = third[i] -
+ * (e(second_i, [s2_i]) e(weighted_first_i - 2B s1_i (second_i - pdk), DK_i/(2B))
+ *  e(first_i, mix_i) - weighted_pairings[i]); neg_scaled_s1 = -(2B s1_i), B Fr. */
+int32_t wbte_pfe_open(wbte_ctx *ctx, void *messages, const void *first, const void *second, const void *third,
+                      const void *weighted_first, const void *weighted_pairings, const void *pre_decryption_key,
+                      const void *neg_scaled_s1, const void *key_lines, const void *generator_lines,
+                      const void *mix_lines, uint64_t B);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1369,4 +1369,194 @@ int32_t wbte_wpfe_open(wbte_ctx* ctx, void* messages, const void* sigmas, uint64
     return c.finish();
 }
 
+// ------------------------------------------------------------------ pfe
+// Gamma-weighted cyclic convolution of pfe/src/decryption.rs:471-526 on B
+// elements in place: io <- INTT(rem) with rem[i] = c spec[i+1] - spec[i] and
+// spec = NTT(io) * E.  E and cvec hold B Fr each (E[k] = B - 1 - 2k mod r,
+// cvec = B copies of c).  Group elements in affine form; GT in Fp12.
+static void pfe_conv_group(Call& c, Group g, uint8_t* io, const uint8_t* E, const uint8_t* cvec, const int32_t* rot,
+                           const int64_t* offs2, uint64_t B, const uint8_t* tw, const uint8_t* twi) {
+    const size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF, xz = g == GROUP_G1 ? G1_XYZZ : G2_XYZZ;
+    uint8_t* work = c.alloc(xz * B);
+    uint8_t* a = c.alloc(aff * B);
+    uint8_t* b = c.alloc(aff * B);
+    uint8_t* pairs = c.alloc(2 * aff * B);
+    if (!c.ok()) return;
+    if (B > 1) launch_group_ntt(g, io, work, tw, (int64_t)B, c.s);
+    launch_mul_batch(g, a, io, 1, E, (int64_t)B, c.s);
+    launch_gather(b, a, rot, (int64_t)B, aff, c.s);
+    launch_mul_batch(g, b, b, 1, cvec, (int64_t)B, c.s);
+    launch_negate(g, a, a, (int64_t)B, c.s);
+    cudaMemcpy2DAsync(pairs, 2 * aff, b, aff, aff, B, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(pairs + aff, 2 * aff, a, aff, aff, B, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(g, io, pairs, offs2, (int64_t)B, c.s);
+    if (B > 1) launch_group_ntt(g, io, work, twi, (int64_t)B, c.s);
+}
+static void pfe_conv_gt(Call& c, uint8_t* io, const uint8_t* E, const uint8_t* cvec, const int32_t* rot, uint64_t B,
+                        const uint8_t* tw, const uint8_t* twi) {
+    uint8_t* a = c.alloc(GT_SZ * B);
+    uint8_t* b = c.alloc(GT_SZ * B);
+    uint8_t* h = c.alloc(GT_SZ * B);
+    if (!c.ok()) return;
+    if (B > 1) launch_gt_ntt(io, tw, (int64_t)B, c.s);
+    launch_gt_pow(a, io, 1, E, (int64_t)B, c.s);
+    launch_gather(h, a, rot, (int64_t)B, GT_SZ, c.s);
+    launch_gt_pow(b, h, 1, cvec, (int64_t)B, c.s);
+    launch_fp12_mul(io, b, 1, a, 1, true, (int64_t)B, c.s);
+    if (B > 1) launch_gt_ntt(io, twi, (int64_t)B, c.s);
+}
+
+struct PfeConvTables {
+    std::vector<int32_t> rot;
+    std::vector<int64_t> offs2;
+    explicit PfeConvTables(uint64_t B) : rot(B), offs2(B + 1) {
+        for (uint64_t i = 0; i < B; i++) rot[i] = (int32_t)((i + 1) % B);
+        for (uint64_t i = 0; i <= B; i++) offs2[i] = (int64_t)(2 * i);
+    }
+};
+
+int32_t wbte_pfe_kernel(wbte_ctx* ctx, const void* fraction_keys, const void* key_sum, uint64_t B, const void* scalars,
+                        void* key_lines, void* generator_lines, void* mix_lines, void* scaled_keys, void* generators,
+                        void* mixes) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!fraction_keys || !key_sum || !scalars || !key_lines || !generator_lines || !mix_lines || B == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    if (log2_exact(B) < 0) return c.fail(WBTE_ERR_SIZE, "batch size must be a power of two");
+    const size_t LT = LINE_SZ * LINES_PER_POINT * B;
+    uint8_t* dkl = c.out(key_lines, LT);
+    uint8_t* dgl = c.out(generator_lines, LT);
+    uint8_t* dml = c.out(mix_lines, LT);
+    uint8_t* dsk_out = scaled_keys ? c.out(scaled_keys, G2_AFF * B) : nullptr;
+    uint8_t* dg_out = generators ? c.out(generators, G2_AFF * B) : nullptr;
+    uint8_t* dmx_out = mixes ? c.out(mixes, G2_AFF * B) : nullptr;
+    const uint8_t* dkeys = c.in(fraction_keys, G2_AFF * B);
+    const uint8_t* dsum = c.in(key_sum, G2_AFF);
+    const uint8_t* sc = c.in(scalars, 6 * FR_SZ * B);
+    PfeConvTables tab(B);
+    const int32_t* drot = c.in_vec(tab.rot);
+    const int64_t* doff2 = c.in_vec(tab.offs2);
+    std::vector<int64_t> offs3(B + 1);
+    for (uint64_t i = 0; i <= B; i++) offs3[i] = (int64_t)(3 * i);
+    const int64_t* doff3 = c.in_vec(offs3);
+    uint8_t* sk = c.alloc(G2_AFF * B);
+    uint8_t* wk = c.alloc(G2_AFF * B);
+    uint8_t* gens = c.alloc(G2_AFF * B);
+    uint8_t* t1 = c.alloc(G2_AFF * B);
+    uint8_t* t2 = c.alloc(G2_AFF * B);
+    uint8_t* triples = c.alloc(3 * G2_AFF * B);
+    uint8_t* mx = c.alloc(G2_AFF * B);
+    const uint8_t* tw = B > 1 ? twiddles(c, (int64_t)B, false) : nullptr;
+    const uint8_t* twi = B > 1 ? twiddles(c, (int64_t)B, true) : nullptr;
+    if (!c.ok()) return c.finish();
+    const uint8_t *inv2b = sc, *E = sc + FR_SZ * B, *cvec = sc + 2 * FR_SZ * B, *s2 = sc + 3 * FR_SZ * B,
+                  *neg_s2 = sc + 4 * FR_SZ * B, *neg_mix = sc + 5 * FR_SZ * B;
+    // scaled keys DK/(2B), their weighted convolution, generators [s2] G2 (pfe/src/decryption.rs:151-214)
+    launch_mul_batch(GROUP_G2, sk, dkeys, 1, inv2b, (int64_t)B, c.s);
+    cudaMemcpyAsync(wk, sk, G2_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    pfe_conv_group(c, GROUP_G2, wk, E, cvec, drot, doff2, B, tw, twi);
+    launch_mul_generator(GROUP_G2, gens, s2, (int64_t)B, c.s);
+    // final mix = weighted - s2 * key_sum - (s1_bar * opening coefficient) * scaled key (:216-230)
+    launch_mul_batch(GROUP_G2, t1, dsum, 0, neg_s2, (int64_t)B, c.s);
+    launch_mul_batch(GROUP_G2, t2, sk, 1, neg_mix, (int64_t)B, c.s);
+    cudaMemcpy2DAsync(triples, 3 * G2_AFF, wk, G2_AFF, G2_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(triples + G2_AFF, 3 * G2_AFF, t1, G2_AFF, G2_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(triples + 2 * G2_AFF, 3 * G2_AFF, t2, G2_AFF, G2_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(GROUP_G2, mx, triples, doff3, (int64_t)B, c.s);
+    launch_prepare_lines(dkl, sk, (int64_t)B, c.s);
+    launch_prepare_lines(dgl, gens, (int64_t)B, c.s);
+    launch_prepare_lines(dml, mx, (int64_t)B, c.s);
+    if (dsk_out) cudaMemcpyAsync(dsk_out, sk, G2_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    if (dg_out) cudaMemcpyAsync(dg_out, gens, G2_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    if (dmx_out) cudaMemcpyAsync(dmx_out, mx, G2_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    return c.finish();
+}
+
+int32_t wbte_pfe_precompute(wbte_ctx* ctx, void* weighted_first, void* weighted_pairings, const void* first,
+                            const void* key_lines, const void* scalars, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!weighted_first || !weighted_pairings || !first || !key_lines || !scalars || B == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    if (log2_exact(B) < 0) return c.fail(WBTE_ERR_SIZE, "batch size must be a power of two");
+    uint8_t* dwf = c.out(weighted_first, G1_AFF * B);
+    uint8_t* dwp = c.out(weighted_pairings, GT_SZ * B);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint8_t* dkl = c.in(key_lines, LINE_SZ * LINES_PER_POINT * B);
+    const uint8_t* sc = c.in(scalars, 2 * FR_SZ * B);
+    PfeConvTables tab(B);
+    const int32_t* drot = c.in_vec(tab.rot);
+    const int64_t* doff2 = c.in_vec(tab.offs2);
+    uint8_t* x = c.alloc(G1_AFF * B);
+    uint8_t* f = c.alloc(GT_SZ * B);
+    const uint8_t* tw = B > 1 ? twiddles(c, (int64_t)B, false) : nullptr;
+    const uint8_t* twi = B > 1 ? twiddles(c, (int64_t)B, true) : nullptr;
+    if (!c.ok()) return c.finish();
+    const uint8_t *E = sc, *cvec = sc + FR_SZ * B;
+    // weighted convolution of the first components and of e(first_i, DK_i/(2B)) (pfe/src/decryption.rs:259-298)
+    cudaMemcpyAsync(x, dfirst, G1_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    pfe_conv_group(c, GROUP_G1, x, E, cvec, drot, doff2, B, tw, twi);
+    launch_miller_lines(f, dkl, dfirst, (int64_t)B, c.s);
+    launch_final_exp(f, f, (int64_t)B, FE_FULL, c.s);
+    pfe_conv_gt(c, f, E, cvec, drot, B, tw, twi);
+    cudaMemcpyAsync(dwf, x, G1_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpyAsync(dwp, f, GT_SZ * B, cudaMemcpyDeviceToDevice, c.s);
+    return c.finish();
+}
+
+int32_t wbte_pfe_open(wbte_ctx* ctx, void* messages, const void* first, const void* second, const void* third,
+                      const void* weighted_first, const void* weighted_pairings, const void* pre_decryption_key,
+                      const void* neg_scaled_s1, const void* key_lines, const void* generator_lines,
+                      const void* mix_lines, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!messages || !first || !second || !third || !weighted_first || !weighted_pairings || !pre_decryption_key ||
+        !neg_scaled_s1 || !key_lines || !generator_lines || !mix_lines || B == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    const size_t LT = LINE_SZ * LINES_PER_POINT * B;
+    uint8_t* dm = c.out(messages, GT_SZ * B);
+    const uint8_t* d1 = c.in(first, G1_AFF * B);
+    const uint8_t* d2 = c.in(second, G1_AFF * B);
+    const uint8_t* d3 = c.in(third, GT_SZ * B);
+    const uint8_t* dwf = c.in(weighted_first, G1_AFF * B);
+    const uint8_t* dwp = c.in(weighted_pairings, GT_SZ * B);
+    const uint8_t* dpdk = c.in(pre_decryption_key, G1_AFF);
+    const uint8_t* ds1 = c.in(neg_scaled_s1, FR_SZ * B);
+    const uint8_t* dkl = c.in(key_lines, LT);
+    const uint8_t* dgl = c.in(generator_lines, LT);
+    const uint8_t* dml = c.in(mix_lines, LT);
+    PfeConvTables tab(B);
+    const int64_t* doff2 = c.in_vec(tab.offs2);
+    std::vector<int32_t> zero(B, 0);
+    const int32_t* dz = c.in_vec(zero);
+    uint8_t* npdk = c.alloc(G1_AFF * B);
+    uint8_t* pairs = c.alloc(2 * G1_AFF * B);
+    uint8_t* d = c.alloc(G1_AFF * B);
+    uint8_t* b1 = c.alloc(G1_AFF * B);
+    uint8_t* f0 = c.alloc(GT_SZ * B);
+    uint8_t* f1 = c.alloc(GT_SZ * B);
+    uint8_t* f2 = c.alloc(GT_SZ * B);
+    if (!c.ok()) return c.finish();
+    // b1_i = weighted_first_i - 2B s1_i (second_i - pdk) (pfe/src/decryption.rs:434-447)
+    launch_gather(npdk, dpdk, dz, (int64_t)B, G1_AFF, c.s);
+    launch_negate(GROUP_G1, npdk, npdk, (int64_t)B, c.s);
+    cudaMemcpy2DAsync(pairs, 2 * G1_AFF, d2, G1_AFF, G1_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(pairs + G1_AFF, 2 * G1_AFF, npdk, G1_AFF, G1_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(GROUP_G1, d, pairs, doff2, (int64_t)B, c.s);
+    launch_mul_batch(GROUP_G1, d, d, 1, ds1, (int64_t)B, c.s);
+    cudaMemcpy2DAsync(pairs, 2 * G1_AFF, dwf, G1_AFF, G1_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(pairs + G1_AFF, 2 * G1_AFF, d, G1_AFF, G1_AFF, B, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(GROUP_G1, b1, pairs, doff2, (int64_t)B, c.s);
+    // mask_i = e(second_i, [s2]) e(b1_i, DK_i/(2B)) e(first_i, mix_i) / weighted_pairings_i (:449-465)
+    launch_miller_lines(f0, dgl, d2, (int64_t)B, c.s);
+    launch_miller_lines(f1, dkl, b1, (int64_t)B, c.s);
+    launch_miller_lines(f2, dml, d1, (int64_t)B, c.s);
+    launch_fp12_mul(f0, f0, 1, f1, 1, false, (int64_t)B, c.s);
+    launch_fp12_mul(f0, f0, 1, f2, 1, false, (int64_t)B, c.s);
+    launch_final_exp(f0, f0, (int64_t)B, FE_FULL, c.s);
+    launch_fp12_mul(f0, f0, 1, dwp, 1, true, (int64_t)B, c.s);
+    launch_fp12_mul(dm, d3, 1, f0, 1, true, (int64_t)B, c.s);
+    return c.finish();
+}
+
 }  // extern "C"
