@@ -43,6 +43,10 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# The batched form runs one CUDA stream per concurrent batch; CUDA maps streams
+# onto this many hardware work queues (default 8), so more streams than queues
+# serialise.  Read once, when the CUDA context is created.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # Fp multiplication in the 12-limb CIOS kernel: 12 rows x (24 products for
@@ -65,7 +69,7 @@ def parse_args():
                     help="batch size of the bounded CPU-oracle sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--concurrency", type=int, default=8, help="concurrent batches (streams) of the batched form")
+    ap.add_argument("--concurrency", type=int, default=32, help="concurrent batches (streams) of the batched form")
     return ap.parse_args()
 
 

@@ -8,7 +8,10 @@ precomputation and opening, the sequence of the reference's `decrypt`
 (weighted_btx/src/decryption.rs:698-709) with the partial decryptions of
 weighted_btx/src/decryption.rs:205-233 in front.
 
-Continuous batching: `slots` worker threads each own a CUDA stream.  A
+Continuous batching: `slots` worker threads each own a CUDA stream (CUDA maps
+streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware queues, 8 unless the
+environment sets more before the CUDA context exists; set it to at least
+`slots`).  A
 request is admitted as soon as a slot is free and its device-memory
 estimate fits in what the HBM budget has left; admitted requests run
 concurrently on their slots' streams, so the kernels of several batches
