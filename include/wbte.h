@@ -230,6 +230,26 @@ int32_t wbte_wbtx_precompute(wbte_ctx *ctx, void *beta, const void *kernel_lines
  * weighted_btx/src/decryption.rs:607-695); invalid slots get the identity. */
 int32_t wbte_wbtx_open(wbte_ctx *ctx, void *messages, const void *opening_keys, const void *sigma, uint64_t T,
                        const void *second, const void *beta, const uint8_t *valid, uint64_t batch_size);
+/* The batched form: K batches of one size B and one accepted committee per
+ * call, batch-major arrays (batch b first).  Each is the K-fold version of the
+ * call above it, with every kernel launched once over all K batches:
+ *   partial_decrypt_many  sigma K*T G1, first K*B G1, q T Fr
+ *   verify_shares_many    ok K int32 (one aggregate check per batch), first
+ *                         K*B G1 with the identity at invalid slots, sigma K*T,
+ *                         challenges K*T Fr, party_indices T (host)
+ *   precompute_many       beta K*B GT over the committee's kernel lines
+ *   open_many             messages K*B GT, opening_keys B*T G2 (shared),
+ *                         sigma K*T G1, second/beta K*B GT, valid K*B. */
+int32_t wbte_wbtx_partial_decrypt_many(wbte_ctx *ctx, void *sigma, const void *first, uint64_t batch_size,
+                                       const void *q, uint64_t T, uint64_t K);
+int32_t wbte_wbtx_verify_shares_many(wbte_ctx *ctx, int32_t *ok, const wbte_wbtx_key *key, const void *first,
+                                     uint64_t batch_size, const void *sigma, const int64_t *party_indices,
+                                     const void *challenges, uint64_t T, uint64_t K);
+int32_t wbte_wbtx_precompute_many(wbte_ctx *ctx, void *beta, const void *kernel_lines, const void *first,
+                                  const uint8_t *valid, uint64_t batch_size, uint64_t K);
+int32_t wbte_wbtx_open_many(wbte_ctx *ctx, void *messages, const void *opening_keys, const void *sigma, uint64_t T,
+                            const void *second, const void *beta, const uint8_t *valid, uint64_t batch_size,
+                            uint64_t K);
 /* Public key material of keygen_with_rng (weighted_btx/src/setup.rs:98-233):
  *   verification_keys[i * N + j] = [q_pos[i * N + j]] G2            (i < L)
  *   negative[i * W + w]          = [z[w] q_neg[i * N + owner[w]]] G2 (i < L)

@@ -83,3 +83,42 @@ def test_concurrent_streams_match_sequential(mix):
     outs, ms = serving.run_concurrent(fn, reqs, 4)
     assert ms > 0
     assert outs == [alone(mat, cts, keys) for cts, keys, _ in reqs]
+
+
+def test_grouped_batches_match_one_by_one(mix):
+    """The batched form (every phase launched once for K batches) gives each
+    batch exactly what decrypting it alone gives, invalid slots included."""
+    mat, reqs = mix
+    group = [r for r in reqs if len(r[0]) == 8 and [k.party_index for k in r[1]] == [1, 3]]
+    rng = ChaCha20Rng.seed_from_u64(42)
+    extra = []
+    for i in range(3):
+        msgs = wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(8)])
+        cts = wb.encrypt_many(mat.encryption_key, msgs, rng)
+        if i == 1:
+            bad = cts[5]
+            cts[5] = wb.Ciphertext(bad.first, bad.second, wb.SchnorrProof(bad.proof.commitment,
+                                                                          (bad.proof.response + 1) % wb.R))
+        extra.append((cts, group[0][1], msgs))
+    group = group + extra
+    keys = group[0][1]
+    cache = serving.CommitteeCache(1 << 30)
+    out = serving.decrypt_group(mat.decryption_key, [g[0] for g in group], keys, ChaCha20Rng.seed_from_u64(3), cache)
+    assert out == [alone(mat, cts, keys) for cts, _, _ in group]
+    assert out[len(group) - 2][5] is None and sum(o is None for r in out for o in r) == 1
+    dev = serving.decrypt_group(mat.decryption_key, [wb.CiphertextBatch.upload(g[0]) for g in group], keys,
+                                ChaCha20Rng.seed_from_u64(4), cache, device_output=True)
+    for o, r in zip(dev, out):
+        assert [wb.to_host(o)[576 * i : 576 * (i + 1)] if x is not None else None for i, x in enumerate(r)] == r
+
+
+def test_validate_batches_equals_validate_batch(mix):
+    mat, reqs = mix
+    batches = [r[0] for r in reqs] + [wb.CiphertextBatch.upload(reqs[2][0])]
+    many = wb.validate_batches(mat.decryption_key, batches)
+    for cts, v in zip(batches, many):
+        one = wb.validate_batch(mat.decryption_key, cts)
+        assert v.batch_size() == one.batch_size() and v.digest() == one.digest()
+        assert v.valid_mask() == one.valid_mask()
+        assert wb.to_host(v.first_dev) == wb.to_host(one.first_dev)
+        assert wb.to_host(v.valid_dev) == wb.to_host(one.valid_dev)

@@ -120,6 +120,10 @@ _SIGNATURES = {
     "wbte_wpfe_prepare": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP],
     "wbte_wpfe_precompute": [_VP, _VP, _VP, _VP, _U64],
     "wbte_wpfe_open": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64],
+    "wbte_wbtx_partial_decrypt_many": [_VP, _VP, _U64, _VP, _U64, _U64],
+    "wbte_wbtx_verify_shares_many": [_VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64, _U64],
+    "wbte_wbtx_precompute_many": [_VP, _VP, _VP, _VP, _U64, _U64],
+    "wbte_wbtx_open_many": [_VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64, _U64],
     "wbte_pfe_kernel": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
     "wbte_pfe_precompute": [_VP, _VP, _VP, _VP, _VP, _U64],
     "wbte_pfe_open": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64],

@@ -213,13 +213,15 @@ __device__ __forceinline__ int64_t bitrev64(int64_t i, int bits) {
     return bits ? (int64_t)(__brevll((unsigned long long)i) >> (64 - bits)) : 0;
 }
 
+// count transforms of size n, stored one after another
 template <class F>
-__global__ void k_ntt_load(uint8_t* work, const uint8_t* in, int64_t n, int bits) {
+__global__ void k_ntt_load(uint8_t* work, const uint8_t* in, int64_t n, int bits, int64_t count) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n * count) return;
     using A = Affine<F>;
+    const int64_t q = i / n, j = i % n;
     Xyzz<F> p = from_affine(load_affine(reinterpret_cast<const A*>(in + GroupOf<F>::AFF * i)));
-    store_vec(reinterpret_cast<Xyzz<F>*>(work) + bitrev64(i, bits), p);
+    store_vec(reinterpret_cast<Xyzz<F>*>(work) + q * n + bitrev64(j, bits), p);
 }
 
 // One radix-2 butterfly per group of L lanes (blocks of one warp); twiddle
@@ -236,14 +238,16 @@ WBTE_INL void ntt_part(G1X& out, const G1X& v, const uint64_t d[4], int c) { g1_
 WBTE_INL void ntt_part(G2X& out, const G2X& v, const uint64_t d[4], int c) { g2_mul_lane(out, v, d, c); }
 
 template <class F>
-__global__ void __launch_bounds__(WARP) k_ntt_stage(uint8_t* work, const uint8_t* tw, int64_t n, int64_t half) {
+__global__ void __launch_bounds__(WARP) k_ntt_stage(uint8_t* work, const uint8_t* tw, int64_t n, int64_t half,
+                                                   int64_t count) {
     constexpr int L = NttLanes<F>::L;
     __shared__ Xyzz<F> sh[WARP];
     const int lane = threadIdx.x, c = lane % L;
     const int64_t t = ((int64_t)blockIdx.x * WARP + lane) / L;
-    const bool active = t < n / 2;
-    const int64_t chunk = active ? t / half : 0, j = active ? t % half : 0;
-    const int64_t a = chunk * 2 * half + j, b = a + half;
+    const bool active = t < (n / 2) * count;
+    const int64_t q = active ? t / (n / 2) : 0, tt = active ? t % (n / 2) : 0;
+    const int64_t chunk = tt / half, j = tt % half;
+    const int64_t a = q * n + chunk * 2 * half + j, b = a + half;
     Xyzz<F>* w = reinterpret_cast<Xyzz<F>*>(work);
     Xyzz<F> part;
     set_inf(part);
@@ -274,6 +278,48 @@ __global__ void __launch_bounds__(WARP) k_ntt_stage(uint8_t* work, const uint8_t
         if (c == 1) tv = neg(tv);
         store_vec(w + (c == 0 ? a : b), xyzz_add(u, tv));
     }
+}
+
+// MSMs of a few terms (the share checks' per-slot aggregates): out[o] =
+// sum_t scalars[vsel[o] n + t] points[pbase[o] + idx[t]], each term multiplied
+// directly with the lane split of the transforms (L lanes per output, one
+// base-|x| digit group each) and the parts summed across the lanes.  Every
+// output costs L threads; Pippenger's windows and window combine would cost
+// more than the terms themselves at this size.
+template <class F>
+__global__ void __launch_bounds__(WARP) k_small_msm(uint8_t* out, const uint8_t* points, const int64_t* pbase,
+                                                   const int32_t* idx, const uint8_t* scalars, const int32_t* vsel,
+                                                   int64_t k, int64_t n) {
+    constexpr int L = NttLanes<F>::L;
+    using A = Affine<F>;
+    __shared__ Xyzz<F> sh[WARP];
+    const int lane = threadIdx.x, c = lane % L;
+    const int64_t o = ((int64_t)blockIdx.x * WARP + lane) / L;
+    const bool active = o < k;
+    Xyzz<F> acc;
+    set_inf(acc);
+    if (active) {
+        const int64_t v = vsel ? (int64_t)vsel[o] : 0;
+        const A* P = reinterpret_cast<const A*>(points) + pbase[o];
+        for (int64_t t = 0; t < n; t++) {
+            Xyzz<F> base = from_affine(load_affine(P + (idx ? (int64_t)idx[t] : t)));
+            uint32_t s[8];
+            load_scalar(s, scalars + FR_SZ * (v * n + t));
+            uint64_t d[4];
+            decompose_base_x(d, s);
+            Xyzz<F> part;
+            ntt_part(part, base, d, c);
+            acc = xyzz_add(acc, part);
+        }
+    }
+    store_vec(sh + lane, acc);
+    __syncwarp();
+    for (int step = 1; step < L; step *= 2) {
+        if (c % (2 * step) == 0) store_vec(sh + lane, xyzz_add(load_vec(sh + lane), load_vec(sh + lane + step)));
+        __syncwarp();
+    }
+    if (active && c == 0)
+        store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * o), to_affine(load_vec(sh + lane)));
 }
 
 template <class F>
@@ -500,30 +546,42 @@ void launch_negate(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStre
     else k_negate<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, in, n);
 }
 
-void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, int64_t n, cudaStream_t s) {
+void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, int64_t n, cudaStream_t s, int64_t count) {
     ProfScope prof_(g == GROUP_G1 ? "ntt_g1" : "ntt_g2", s);
-    if (n <= 0) return;
+    if (n <= 0 || count <= 0) return;
     int bits = 0;
     while ((int64_t(1) << bits) < n) bits++;
+    const int64_t total = n * count, butterflies = (n / 2) * count;
     if (g == GROUP_G1) {
         note_launch();
-        k_ntt_load<Fp><<<blocks_for(n), TPB, 0, s>>>(work, io, n, bits);
+        k_ntt_load<Fp><<<blocks_for(total), TPB, 0, s>>>(work, io, n, bits, count);
         for (int64_t half = 1; half < n; half *= 2) {
             note_launch();
-            k_ntt_stage<Fp><<<blocks_for(NttLanes<Fp>::L * (n / 2), WARP), WARP, 0, s>>>(work, tw, n, half);
+            k_ntt_stage<Fp><<<blocks_for(NttLanes<Fp>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
         }
         note_launch();
-        k_xyzz_to_affine<Fp><<<blocks_for(n), TPB, 0, s>>>(io, work, n);
+        k_xyzz_to_affine<Fp><<<blocks_for(total), TPB, 0, s>>>(io, work, total);
     } else {
         note_launch();
-        k_ntt_load<Fp2><<<blocks_for(n), TPB, 0, s>>>(work, io, n, bits);
+        k_ntt_load<Fp2><<<blocks_for(total), TPB, 0, s>>>(work, io, n, bits, count);
         for (int64_t half = 1; half < n; half *= 2) {
             note_launch();
-            k_ntt_stage<Fp2><<<blocks_for(NttLanes<Fp2>::L * (n / 2), WARP), WARP, 0, s>>>(work, tw, n, half);
+            k_ntt_stage<Fp2><<<blocks_for(NttLanes<Fp2>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
         }
         note_launch();
-        k_xyzz_to_affine<Fp2><<<blocks_for(n), TPB, 0, s>>>(io, work, n);
+        k_xyzz_to_affine<Fp2><<<blocks_for(total), TPB, 0, s>>>(io, work, total);
     }
+}
+
+void launch_small_msm(Group g, uint8_t* out, const uint8_t* points, const int64_t* pbase, const int32_t* idx,
+                      const uint8_t* scalars, const int32_t* vsel, int64_t k, int64_t n, cudaStream_t s) {
+    ProfScope prof_(g == GROUP_G1 ? "small_msm_g1" : "small_msm_g2", s);
+    if (k <= 0) return;
+    note_launch();
+    if (g == GROUP_G1)
+        k_small_msm<Fp><<<blocks_for(NttLanes<Fp>::L * k, WARP), WARP, 0, s>>>(out, points, pbase, idx, scalars, vsel, k, n);
+    else
+        k_small_msm<Fp2><<<blocks_for(NttLanes<Fp2>::L * k, WARP), WARP, 0, s>>>(out, points, pbase, idx, scalars, vsel, k, n);
 }
 
 void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {

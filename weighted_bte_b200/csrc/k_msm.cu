@@ -341,6 +341,10 @@ void launch_msm_family(Group g, uint8_t* out, const uint8_t* points, const int64
         cudaMemsetAsync(out, 0, (g == GROUP_G1 ? G1_AFF : G2_AFF) * (size_t)k, s);
         return;
     }
+    if (!forced && n <= SMALL_MSM_MAX) {
+        launch_small_msm(g, out, points, pbase, idx, scalars, vsel, k, n, s);
+        return;
+    }
     MsmPlan p = forced ? *forced : msm_plan(g, n, k);
     size_t bytes = msm_family_scratch_bytes(g, V, k, n, p);
     void* scratch = nullptr;

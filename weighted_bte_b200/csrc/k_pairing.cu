@@ -32,20 +32,21 @@ __global__ void k_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n) {
     }
 }
 
-__global__ void k_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n) {
+// pair i uses line table i % lines_n (tables stored line-major, stride lines_n)
+__global__ void k_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t lines_n) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     G1A P = load_affine(reinterpret_cast<const G1A*>(p + G1_AFF * i));
     Fp12 f;
-    miller_loop_lines(f, reinterpret_cast<const Line*>(lines) + i, (size_t)n, P);
+    miller_loop_lines(f, reinterpret_cast<const Line*>(lines) + i % lines_n, (size_t)lines_n, P);
     store_vec(as_gt(out) + i, f);
 }
 
-__global__ void k_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, int64_t p_mod) {
+__global__ void k_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, int64_t p_mod, int64_t q_mod) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     G1A P = load_affine(reinterpret_cast<const G1A*>(p + G1_AFF * (p_mod ? i % p_mod : i)));
-    G2A Q = load_affine(reinterpret_cast<const G2A*>(q + G2_AFF * i));
+    G2A Q = load_affine(reinterpret_cast<const G2A*>(q + G2_AFF * (q_mod ? i % q_mod : i)));
     Fp12 f;
     miller_loop(f, P, Q);
     store_vec(as_gt(out) + i, f);
@@ -81,10 +82,11 @@ __device__ __forceinline__ int64_t bitrev64(int64_t i, int bits) {
     return bits ? (int64_t)(__brevll((unsigned long long)i) >> (64 - bits)) : 0;
 }
 
-__global__ void k_gt_bitrev(uint8_t* dst, const uint8_t* src, int64_t n, int bits) {
+__global__ void k_gt_bitrev(uint8_t* dst, const uint8_t* src, int64_t n, int bits, int64_t count) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    store_vec(as_gt(dst) + bitrev64(i, bits), load_vec(as_gt(src) + i));
+    if (i >= n * count) return;
+    const int64_t q = i / n, j = i % n;
+    store_vec(as_gt(dst) + q * n + bitrev64(j, bits), load_vec(as_gt(src) + i));
 }
 
 // The GT transforms and GT exponentiation split each exponentiation v^s over
@@ -121,13 +123,15 @@ WBTE_INL void gt_combine(Fp12* sh, int lane, int c) {
 
 // One butterfly per group of lanes: u' = u t, v' = u t^-1 with t = v^tw
 // (inverse by conjugation in the cyclotomic subgroup).
-__global__ void __launch_bounds__(WARP) k_gt_stage(uint8_t* io, const uint8_t* tw, int64_t n, int64_t half) {
+__global__ void __launch_bounds__(WARP) k_gt_stage(uint8_t* io, const uint8_t* tw, int64_t n, int64_t half,
+                                                  int64_t count) {
     __shared__ Fp12 sh[WARP];
     const int lane = threadIdx.x, c = lane % GT_LANES;
     const int64_t t = ((int64_t)blockIdx.x * WARP + lane) / GT_LANES;
-    const bool active = t < n / 2;
-    const int64_t chunk = active ? t / half : 0, j = active ? t % half : 0;
-    const int64_t a = chunk * 2 * half + j, b = a + half;
+    const bool active = t < (n / 2) * count;
+    const int64_t q = active ? t / (n / 2) : 0, tt = active ? t % (n / 2) : 0;
+    const int64_t chunk = tt / half, j = tt % half;
+    const int64_t a = q * n + chunk * 2 * half + j, b = a + half;
     Fp12 part = fp12_one();
     if (active) {
         Fp12 v = load_vec(as_gt(io) + b);
@@ -149,24 +153,27 @@ __global__ void __launch_bounds__(WARP) k_gt_stage(uint8_t* io, const uint8_t* t
 }
 
 // last stage keeping only the first out_count outputs
-__global__ void __launch_bounds__(WARP) k_gt_last_prefix(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count) {
+__global__ void __launch_bounds__(WARP) k_gt_last_prefix(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count,
+                                                        int64_t count) {
     __shared__ Fp12 sh[WARP];
     const int lane = threadIdx.x, c = lane % GT_LANES;
-    const int64_t j = ((int64_t)blockIdx.x * WARP + lane) / GT_LANES;
-    const bool active = j < out_count;
+    const int64_t jj = ((int64_t)blockIdx.x * WARP + lane) / GT_LANES;
+    const bool active = jj < out_count * count;
+    const int64_t q = active ? jj / out_count : 0, j = active ? jj % out_count : 0;
     const int64_t half = n / 2;
+    Fp12* base = as_gt(io) + q * n;
     Fp12 part = fp12_one();
     if (active) {
-        Fp12 v = load_vec(as_gt(io) + half + j);
+        Fp12 v = load_vec(base + half + j);
         if (j != 0) gt_pow_part(part, v, tw + FR_SZ * j, c);
         else if (c == 0) part = v;
     }
     store_vec(sh + lane, part);
     gt_combine(sh, lane, c);
     if (active && c == 0) {
-        Fp12 u = load_vec(as_gt(io) + j), tv = load_vec(sh + lane);
+        Fp12 u = load_vec(base + j), tv = load_vec(sh + lane);
         fp12_mul(u, u, tv);
-        store_vec(as_gt(io) + j, u);
+        store_vec(base + j, u);
     }
 }
 
@@ -263,17 +270,19 @@ void launch_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n, cudaStrea
     note_launch();
     k_prepare_lines<<<blocks_for(n), TPB, 0, s>>>(lines, q, n);
 }
-void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, cudaStream_t s) {
+void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, cudaStream_t s,
+                         int64_t lines_n) {
     ProfScope prof_("miller_lines", s);
     if (n <= 0) return;
     note_launch();
-    k_miller_lines<<<blocks_for(n), TPB, 0, s>>>(out, lines, p, n);
+    k_miller_lines<<<blocks_for(n), TPB, 0, s>>>(out, lines, p, n, lines_n > 0 ? lines_n : n);
 }
-void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, cudaStream_t s, int64_t p_mod) {
+void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, cudaStream_t s, int64_t p_mod,
+                   int64_t q_mod) {
     ProfScope prof_("miller", s);
     if (n <= 0) return;
     note_launch();
-    k_miller<<<blocks_for(n), TPB, 0, s>>>(out, p, q, n, p_mod);
+    k_miller<<<blocks_for(n), TPB, 0, s>>>(out, p, q, n, p_mod, q_mod);
 }
 void launch_fp12_mask(uint8_t* io, const uint8_t* valid, int64_t n, cudaStream_t s) {
     if (n <= 0) return;
@@ -293,31 +302,35 @@ void launch_final_exp(uint8_t* out, const uint8_t* in, int64_t n, FinalExpMode m
     k_final_exp<<<blocks_for(n), TPB, 0, s>>>(out, in, n, (int)mode);
 }
 
-static void gt_transform(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count, bool prefix, cudaStream_t s) {
+static void gt_transform(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count, bool prefix, cudaStream_t s,
+                         int64_t count) {
     ProfScope prof_("gt_ifft", s);
-    if (n <= 1) return;
+    if (n <= 1 || count <= 0) return;
     int bits = 0;
     while ((int64_t(1) << bits) < n) bits++;
     uint8_t* tmp = nullptr;
-    if (cudaMallocAsync(&tmp, GT_SZ * (size_t)n, s) != cudaSuccess) return;
+    if (cudaMallocAsync(&tmp, GT_SZ * (size_t)(n * count), s) != cudaSuccess) return;
     note_launch();
-    k_gt_bitrev<<<blocks_for(n), TPB, 0, s>>>(tmp, io, n, bits);
+    k_gt_bitrev<<<blocks_for(n * count), TPB, 0, s>>>(tmp, io, n, bits, count);
     int64_t last_half = prefix ? n / 4 : n / 2;
     for (int64_t half = 1; half <= last_half; half *= 2) {
         note_launch();
-        k_gt_stage<<<blocks_for(GT_LANES * (n / 2), WARP), WARP, 0, s>>>(tmp, tw, n, half);
+        k_gt_stage<<<blocks_for(GT_LANES * (n / 2) * count, WARP), WARP, 0, s>>>(tmp, tw, n, half, count);
     }
     if (prefix && out_count > 0) {
         note_launch();
-        k_gt_last_prefix<<<blocks_for(GT_LANES * out_count, WARP), WARP, 0, s>>>(tmp, tw, n, out_count);
+        k_gt_last_prefix<<<blocks_for(GT_LANES * out_count * count, WARP), WARP, 0, s>>>(tmp, tw, n, out_count, count);
     }
-    cudaMemcpyAsync(io, tmp, GT_SZ * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(io, tmp, GT_SZ * (size_t)(n * count), cudaMemcpyDeviceToDevice, s);
     cudaFreeAsync(tmp, s);
 }
-void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* tw_inv, int64_t n, int64_t out_count, cudaStream_t s) {
-    gt_transform(io, tw_inv, n, out_count, true, s);
+void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* tw_inv, int64_t n, int64_t out_count, cudaStream_t s,
+                                   int64_t count) {
+    gt_transform(io, tw_inv, n, out_count, true, s, count);
 }
-void launch_gt_ntt(uint8_t* io, const uint8_t* tw, int64_t n, cudaStream_t s) { gt_transform(io, tw, n, n, false, s); }
+void launch_gt_ntt(uint8_t* io, const uint8_t* tw, int64_t n, cudaStream_t s, int64_t count) {
+    gt_transform(io, tw, n, n, false, s, count);
+}
 
 void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint8_t* scalars, int64_t n, cudaStream_t s) {
     ProfScope prof_("gt_pow", s);

@@ -67,7 +67,8 @@ void launch_mul_pow2(Group g, uint8_t* out, const uint8_t* in, int64_t n, int k,
 void launch_segment_sum(Group g, uint8_t* out, const uint8_t* in, const int64_t* offsets, int64_t k, cudaStream_t s);
 void launch_negate(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
 // radix-2 DIT transform of n affine points in place (forward or unscaled inverse)
-void launch_group_ntt(Group g, uint8_t* io_affine, uint8_t* work_xyzz, const uint8_t* twiddles, int64_t n, cudaStream_t s);
+void launch_group_ntt(Group g, uint8_t* io_affine, uint8_t* work_xyzz, const uint8_t* twiddles, int64_t n, cudaStream_t s,
+                      int64_t count = 1);
 // compressed (ZCash) encodings
 void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
 // valid[i] = ([s_i] G == R_i + [c_i] X_i), G the G1 generator
@@ -83,6 +84,11 @@ struct MsmPlan {
     int64_t segment = 0, segments = 0;
 };
 MsmPlan msm_plan(Group g, int64_t n, int64_t k);
+// MSMs of at most SMALL_MSM_MAX terms, computed term by term with lane-split
+// scalar multiplication (launch_msm_family dispatches here).
+constexpr int64_t SMALL_MSM_MAX = 4;
+void launch_small_msm(Group g, uint8_t* out, const uint8_t* points, const int64_t* pbase, const int32_t* idx,
+                      const uint8_t* scalars, const int32_t* vsel, int64_t k, int64_t n, cudaStream_t s);
 void launch_msm_family(Group g, uint8_t* out, const uint8_t* points, const int64_t* pbase, const int32_t* idx,
                        const uint8_t* scalars, const int32_t* vsel, int32_t V, int64_t k, int64_t n,
                        cudaStream_t s, const MsmPlan* forced = nullptr);
@@ -96,9 +102,12 @@ void launch_msm_family_scratch(Group g, uint8_t* out, const uint8_t* points, con
 // lines[step * n + i] for step < 68: prepared line coefficients of q[i]
 void launch_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n, cudaStream_t s);
 // out[i] = Miller(p[i], lines of pair i), lines laid out as above with n pairs
-void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, cudaStream_t s);
+void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, cudaStream_t s,
+                         int64_t lines_n = 0);
 // out[i] = Miller(p[p_mod ? i % p_mod : i], q[i])
-void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, cudaStream_t s, int64_t p_mod = 0);
+// pair i: P[p_mod ? i % p_mod : i], Q[q_mod ? i % q_mod : i]
+void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, cudaStream_t s, int64_t p_mod = 0,
+                   int64_t q_mod = 0);
 // io[i] = 1 where valid[i] == 0
 void launch_fp12_mask(uint8_t* io, const uint8_t* valid, int64_t n, cudaStream_t s);
 // out[j] = product of in[offsets[j] .. offsets[j+1])
@@ -106,9 +115,10 @@ void launch_fp12_segment_product(uint8_t* out, const uint8_t* in, const int64_t*
 enum FinalExpMode : int { FE_FULL = 0, FE_EASY = 1, FE_HARD = 2 };
 void launch_final_exp(uint8_t* out, const uint8_t* in, int64_t n, FinalExpMode mode, cudaStream_t s);
 // unscaled inverse transform over cyclotomic values keeping out_count outputs
-void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* twiddles_inv, int64_t n, int64_t out_count, cudaStream_t s);
+void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* twiddles_inv, int64_t n, int64_t out_count, cudaStream_t s,
+                                   int64_t count = 1);
 // full unscaled transform over GT values (forward if twiddles are powers of w, inverse with w^-1)
-void launch_gt_ntt(uint8_t* io, const uint8_t* twiddles, int64_t n, cudaStream_t s);
+void launch_gt_ntt(uint8_t* io, const uint8_t* twiddles, int64_t n, cudaStream_t s, int64_t count = 1);
 // out[i] = base[i * stride]^scalars[i] on GT
 void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t base_stride, const uint8_t* scalars, int64_t n, cudaStream_t s);
 // out[i] = a[i * sa] * b[i * sb] (conj_b: b conjugated)

@@ -1559,4 +1559,172 @@ int32_t wbte_pfe_open(wbte_ctx* ctx, void* messages, const void* first, const vo
     return c.finish();
 }
 
+// ------------------------------------------- weighted_btx, K batches per call
+// The batched form: K batches of the same size B and the same accepted
+// committee go through each phase in one launch sequence, so every kernel
+// sees K times the work of one batch.  Arrays are batch-major (batch q first).
+int32_t wbte_wbtx_partial_decrypt_many(wbte_ctx* ctx, void* sigma, const void* first, uint64_t B, const void* q,
+                                       uint64_t T, uint64_t K) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (T == 0 || K == 0) return c.finish();
+    if (!sigma || !first || !q || B == 0) return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    uint8_t* dsig = c.out(sigma, G1_AFF * T * K);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B * K);
+    const uint8_t* dq = c.in(q, FR_SZ * T);
+    uint8_t* scalars = c.alloc(FR_SZ * T * B);
+    std::vector<int64_t> base(T * K);
+    std::vector<int32_t> vsel(T * K);
+    for (uint64_t b = 0; b < K; b++)
+        for (uint64_t j = 0; j < T; j++) {
+            base[b * T + j] = (int64_t)(b * B);
+            vsel[b * T + j] = (int32_t)j;
+        }
+    const int64_t* db = c.in_vec(base);
+    const int32_t* dv = c.in_vec(vsel);
+    if (!c.ok()) return c.finish();
+    // sigma[b T + j] = sum_i q_j^(i+1) first[b B + i] (weighted_btx/src/decryption.rs:205-233)
+    for (uint64_t j = 0; j < T; j++) launch_fr_powers(scalars + FR_SZ * B * j, dq + FR_SZ * j, (int64_t)B, 1, c.s);
+    launch_msm_family(GROUP_G1, dsig, dfirst, db, nullptr, scalars, dv, (int32_t)T, (int64_t)(T * K), (int64_t)B, c.s);
+    return c.finish();
+}
+
+int32_t wbte_wbtx_verify_shares_many(wbte_ctx* ctx, int32_t* ok, const wbte_wbtx_key* key, const void* first, uint64_t B,
+                                     const void* sigma, const int64_t* party_indices, const void* challenges,
+                                     uint64_t T, uint64_t K) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!ok) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    for (uint64_t b = 0; b < K; b++) ok[b] = 0;
+    if (check_key(c, key)) return c.finish();
+    if (K == 0) return c.finish();
+    if (T == 0) {
+        for (uint64_t b = 0; b < K; b++) ok[b] = 1;
+        return c.finish();
+    }
+    if (!first || !sigma || !party_indices || !challenges) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    if (B == 0 || B > key->max_batch_size) return c.fail(WBTE_ERR_SIZE, "batch size out of range");
+    const uint64_t N = key->party_count, P1 = B + 1;
+    std::vector<int32_t> pidx(T);
+    for (uint64_t j = 0; j < T; j++) {
+        if (party_indices[j] < 0 || (uint64_t)party_indices[j] >= N) return c.fail(WBTE_ERR_INVALID_ARG, "invalid party index");
+        pidx[j] = (int32_t)party_indices[j];
+    }
+    // first carries the identity at invalid slots, whose pairings are 1, so
+    // every slot enters the product (weighted_btx/src/decryption.rs:358-422)
+    const uint8_t* dfirst = c.in(first, G1_AFF * B * K);
+    const uint8_t* dsig = c.in(sigma, G1_AFF * T * K);
+    const uint8_t* dch = c.in(challenges, FR_SZ * T * K);
+    const uint8_t* dvk = c.in(key->verification_keys, G2_AFF * key->max_batch_size * N);
+    uint8_t* agg = c.alloc(G1_AFF * K);
+    uint8_t* aggvk = c.alloc(G2_AFF * B * K);
+    uint8_t* P = c.alloc(G1_AFF * P1 * K);
+    uint8_t* Q = c.alloc(G2_AFF * P1 * K);
+    uint8_t* f = c.alloc(GT_SZ * P1 * K);
+    uint8_t* prod = c.alloc(GT_SZ * K);
+    uint8_t* flags = c.alloc(K);
+    std::vector<int64_t> sbase(K), vbase(B * K), offs(K + 1);
+    std::vector<int32_t> svsel(K), vvsel(B * K), gidx(K, 0);
+    for (uint64_t b = 0; b < K; b++) {
+        sbase[b] = (int64_t)(b * T);
+        svsel[b] = (int32_t)b;
+        for (uint64_t i = 0; i < B; i++) {
+            vbase[b * B + i] = (int64_t)(i * N);
+            vvsel[b * B + i] = (int32_t)b;
+        }
+    }
+    for (uint64_t b = 0; b <= K; b++) offs[b] = (int64_t)(b * P1);
+    const int64_t* dsbase = c.in_vec(sbase);
+    const int32_t* dsvsel = c.in_vec(svsel);
+    const int64_t* dvbase = c.in_vec(vbase);
+    const int32_t* dvvsel = c.in_vec(vvsel);
+    const int32_t* dpidx = c.in_vec(pidx);
+    const int32_t* dgidx = c.in_vec(gidx);
+    const int64_t* doffs = c.in_vec(offs);
+    uint8_t* g2 = g2_generator_dev(c);
+    if (!c.ok()) return c.finish();
+    launch_msm_family(GROUP_G1, agg, dsig, dsbase, nullptr, dch, dsvsel, (int32_t)K, (int64_t)K, (int64_t)T, c.s);
+    launch_negate(GROUP_G1, agg, agg, (int64_t)K, c.s);
+    launch_msm_family(GROUP_G2, aggvk, dvk, dvbase, dpidx, dch, dvvsel, (int32_t)K, (int64_t)(B * K), (int64_t)T, c.s);
+    cudaMemcpy2DAsync(P, G1_AFF * P1, dfirst, G1_AFF * B, G1_AFF * B, K, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(P + G1_AFF * B, G1_AFF * P1, agg, G1_AFF, G1_AFF, K, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(Q, G2_AFF * P1, aggvk, G2_AFF * B, G2_AFF * B, K, cudaMemcpyDeviceToDevice, c.s);
+    uint8_t* gcol = c.alloc(G2_AFF * K);
+    if (!c.ok()) return c.finish();
+    launch_gather(gcol, g2, dgidx, (int64_t)K, G2_AFF, c.s);
+    cudaMemcpy2DAsync(Q + G2_AFF * B, G2_AFF * P1, gcol, G2_AFF, G2_AFF, K, cudaMemcpyDeviceToDevice, c.s);
+    launch_miller(f, P, Q, (int64_t)(P1 * K), c.s);
+    launch_fp12_segment_product(prod, f, doffs, (int64_t)K, c.s);
+    launch_final_exp(prod, prod, (int64_t)K, FE_FULL, c.s);
+    launch_fp12_is_one(flags, prod, (int64_t)K, c.s);
+    std::vector<uint8_t> h(K);
+    if (c.to_host(h.data(), flags, K))
+        for (uint64_t b = 0; b < K; b++) ok[b] = h[b] ? 1 : 0;
+    return c.finish();
+}
+
+int32_t wbte_wbtx_precompute_many(wbte_ctx* ctx, void* beta, const void* kernel_lines, const void* first,
+                                  const uint8_t* valid, uint64_t B, uint64_t K) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!beta || !kernel_lines || !first || !valid || B == 0 || K == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    const uint64_t m = next_pow2(2 * B);
+    uint8_t* dbeta = c.out(beta, GT_SZ * B * K);
+    const uint8_t* dl = c.in(kernel_lines, LINE_SZ * LINES_PER_POINT * m);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B * K);
+    const uint8_t* dvalid = c.in(valid, B * K);
+    uint8_t* x = c.zeros(G1_AFF * m * K);
+    uint8_t* work = c.alloc(G1_XYZZ * m * K);
+    uint8_t* f = c.alloc(GT_SZ * m * K);
+    const uint8_t* tw = twiddles(c, (int64_t)m, false);
+    const uint8_t* twi = twiddles(c, (int64_t)m, true);
+    if (!c.ok()) return c.finish();
+    // per batch: G1 transform of the zero-padded first components, prepared
+    // Miller loops against the shared kernel lines, easy part, truncated
+    // cyclotomic inverse transform, hard part (weighted_btx/src/decryption.rs:555-603)
+    cudaMemcpy2DAsync(x, G1_AFF * m, dfirst, G1_AFF * B, G1_AFF * B, K, cudaMemcpyDeviceToDevice, c.s);
+    launch_group_ntt(GROUP_G1, x, work, tw, (int64_t)m, c.s, (int64_t)K);
+    launch_miller_lines(f, dl, x, (int64_t)(m * K), c.s, (int64_t)m);
+    launch_final_exp(f, f, (int64_t)(m * K), FE_EASY, c.s);
+    launch_cyclotomic_prefix_ifft(f, twi, (int64_t)m, (int64_t)B, c.s, (int64_t)K);
+    cudaMemcpy2DAsync(dbeta, GT_SZ * B, f, GT_SZ * m, GT_SZ * B, K, cudaMemcpyDeviceToDevice, c.s);
+    launch_final_exp(dbeta, dbeta, (int64_t)(B * K), FE_HARD, c.s);
+    launch_fp12_mask(dbeta, dvalid, (int64_t)(B * K), c.s);
+    return c.finish();
+}
+
+int32_t wbte_wbtx_open_many(wbte_ctx* ctx, void* messages, const void* opening_keys, const void* sigma, uint64_t T,
+                            const void* second, const void* beta, const uint8_t* valid, uint64_t B, uint64_t K) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!messages || !opening_keys || !sigma || !second || !beta || !valid || B == 0 || T == 0 || K == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    uint8_t* dm = c.out(messages, GT_SZ * B * K);
+    const uint8_t* dk = c.in(opening_keys, G2_AFF * B * T);
+    const uint8_t* ds = c.in(sigma, G1_AFF * T * K);
+    const uint8_t* d2 = c.in(second, GT_SZ * B * K);
+    const uint8_t* db = c.in(beta, GT_SZ * B * K);
+    const uint8_t* dv = c.in(valid, B * K);
+    const uint64_t BT = B * T;
+    uint8_t* P = c.alloc(G1_AFF * BT * K);
+    uint8_t* f = c.alloc(GT_SZ * BT * K);
+    uint8_t* alpha = c.alloc(GT_SZ * B * K);
+    std::vector<int32_t> pidx(BT * K);
+    for (uint64_t b = 0; b < K; b++)
+        for (uint64_t x = 0; x < BT; x++) pidx[b * BT + x] = (int32_t)(b * T + x % T);
+    std::vector<int64_t> offs(B * K + 1);
+    for (uint64_t i = 0; i <= B * K; i++) offs[i] = (int64_t)(i * T);
+    const int32_t* dpidx = c.in_vec(pidx);
+    const int64_t* doffs = c.in_vec(offs);
+    if (!c.ok()) return c.finish();
+    // alpha[b B + i] = prod_k e(sigma[b T + k], opening_keys[i T + k]) (weighted_btx/src/decryption.rs:607-695)
+    launch_gather(P, ds, dpidx, (int64_t)(BT * K), G1_AFF, c.s);
+    launch_miller(f, P, dk, (int64_t)(BT * K), c.s, 0, (int64_t)BT);
+    launch_fp12_segment_product(alpha, f, doffs, (int64_t)(B * K), c.s);
+    launch_final_exp(alpha, alpha, (int64_t)(B * K), FE_FULL, c.s);
+    launch_unmask(dm, d2, alpha, db, dv, (int64_t)(B * K), c.s);
+    return c.finish();
+}
+
 }  // extern "C"

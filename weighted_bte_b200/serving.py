@@ -15,7 +15,11 @@ environment sets more before the CUDA context exists; set it to at least
 request is admitted as soon as a slot is free and its device-memory
 estimate fits in what the HBM budget has left; admitted requests run
 concurrently on their slots' streams, so the kernels of several batches
-overlap on the device.  Requests are admitted in arrival order.
+overlap on the device.  Requests are admitted in arrival order.  A slot that
+admits a request also takes the waiting requests of the same batch size and
+committee (up to `max_group`, within the budget) and decrypts them as one
+group: `decrypt_group`, where every GPU phase is one launch over all of
+their batches (the batched form).
 
 Committee cache: the reference documents the committee preparation as
 independent of the ciphertexts and reusable for another batch of the same
@@ -39,6 +43,9 @@ import time
 from dataclasses import dataclass, field
 from typing import Callable, List, Optional, Sequence
 
+import numpy as np
+
+from . import _lib
 from . import weighted_btx as wb
 from .rng import ChaCha20Rng
 
@@ -161,6 +168,68 @@ def decrypt_request(dk: wb.PublicDecryptionKey, ciphertexts, party_keys: Sequenc
     return wb.open_batch(pre, accepted, batch, ciphertexts, cross, device_output=device_output)
 
 
+def decrypt_group(dk: wb.PublicDecryptionKey, batches: Sequence, party_keys: Sequence[wb.PartySecretKey], rng,
+                  cache: Optional[CommitteeCache] = None, device_output: bool = False) -> List:
+    """The batched form: K batches of one size, decrypted by one committee,
+    with every GPU phase launched once for all K (the wbte_wbtx_*_many calls).
+    Per batch the result is exactly `decrypt_request`'s: validation,
+    transcripts, digests and the share-acceptance rules run per batch; a batch
+    whose aggregate share check fails falls back to the per-share path alone."""
+    torch = wb._t()
+    K = len(batches)
+    if K == 0:
+        return []
+    B = len(batches[0])
+    if any(len(b) != B for b in batches):
+        raise ValueError("a group holds batches of one size")
+    T = len(party_keys)
+    validated = wb.validate_batches(dk, batches)
+    for pk in party_keys:
+        if pk.setup_id() != dk.setup_id():
+            from . import errors as E
+
+            raise E.MismatchedSetup()
+    first = torch.cat([v.first_dev[: G1B * B] for v in validated])
+    valid = torch.cat([v.valid_dev[:B] for v in validated])
+    ctx = wb._ctx()
+    sig = bytearray(G1B * T * K)
+    ctx.call("wbte_wbtx_partial_decrypt_many", sig, first, B, b"".join(wb.fr_bytes(pk.secret_scalar()) for pk in party_keys),
+             T, K)
+    shares = [[wb.DecryptionShare(pk.party_index, bytes(sig[G1B * (b * T + j) : G1B * (b * T + j + 1)]),
+                                  validated[b].digest(), pk.setup_id()) for j, pk in enumerate(party_keys)]
+              for b in range(K)]
+    screened = [wb.screen_shares(dk, validated[b], shares[b]) for b in range(K)]
+    full = all(len(c) == T and not r for c, r in screened)
+    if full and T > 0:
+        from .rng import sample_nonzero
+
+        challenges = [[sample_nonzero(rng) for _ in range(T)] for _ in range(K)]
+        ok = np.zeros(K, dtype=np.int32)
+        ctx.call("wbte_wbtx_verify_shares_many", ok, dk.abi_key(), first, B, bytes(sig),
+                 _lib.i64_array([pk.party_index for pk in party_keys]),
+                 b"".join(wb.fr_bytes(c) for row in challenges for c in row), T, K)
+        accepted = [wb.finish_acceptance(dk, validated[b], *screened[b], bool(ok[b])) for b in range(K)]
+    else:
+        accepted = [wb.accept_decryption_shares(dk, validated[b], shares[b], rng) for b in range(K)]
+    committees = {tuple(a.party_indices()) for a in accepted}
+    if len(committees) != 1:  # a share was rejected in some batch: decrypt those one by one
+        return [decrypt_request(dk, cts, party_keys, rng, cache, device_output) for cts in batches]
+    pre = cache.get(dk, accepted[0]) if cache is not None else wb.prepare_decryption(dk, accepted[0])
+    Ta = accepted[0].party_count()
+    sigmas = b"".join(s.sigma for a in accepted for s in a.shares())
+    beta = wb.empty_device(GTB * B * K)
+    ctx.call("wbte_wbtx_precompute_many", beta, pre.kernel_lines, first, valid, B, K)
+    second = torch.cat([c.second[: GTB * B] if isinstance(c, wb.CiphertextBatch)
+                        else wb.to_device(b"".join(x.second for x in c)) for c in batches])
+    out = wb.empty_device(GTB * B * K)
+    ctx.call("wbte_wbtx_open_many", out, pre.opening_keys, sigmas, Ta, second, beta, valid, B, K)
+    if device_output:
+        return [out[GTB * B * b : GTB * B * (b + 1)] for b in range(K)]
+    host = wb.to_host(out, GTB * B * K)
+    return [[host[GTB * (b * B + i) : GTB * (b * B + i + 1)] if validated[b].valid[i] else None for i in range(B)]
+            for b in range(K)]
+
+
 @dataclass
 class _Request:
     ciphertexts: object
@@ -181,10 +250,13 @@ class DecryptionServer:
 
     def __init__(self, decryption_key: wb.PublicDecryptionKey, slots: int = 4,
                  hbm_budget_bytes: Optional[int] = None, cache_bytes: Optional[int] = None,
-                 device: int = 0, cache_committees: bool = True):
+                 device: int = 0, cache_committees: bool = True, max_group: int = 1):
         torch = wb._t()
         self.dk = decryption_key
         self.device = device
+        # requests of one batch size and committee that wait together are
+        # decrypted as one group (the batched form), up to max_group at a time
+        self.max_group = max(1, int(max_group))
         if hbm_budget_bytes is None:
             free, _total = torch.cuda.mem_get_info(device)
             hbm_budget_bytes = free // 2
@@ -252,26 +324,46 @@ class DecryptionServer:
                 "peak_in_flight": self.peak_in_flight, "peak_bytes": self.peak_bytes}
 
     # ------------------------------------------------------------ workers
-    def _admit(self) -> Optional[_Request]:
+    @staticmethod
+    def _group_key(req: _Request):
+        return len(req.ciphertexts), tuple(k.party_index for k in req.party_keys)
+
+    def _admit(self) -> Optional[List[_Request]]:
+        """Admit the head request once it fits the budget, then every waiting
+        request of the same batch size and committee that still fits, up to
+        max_group (requests keep their arrival order)."""
         with self._cv:
             while True:
                 if self._queue:
                     head = self._queue[0]
                     if self._in_use + head.need <= self.budget:
-                        self._queue.popleft()
-                        self._in_use += head.need
-                        self.peak_bytes = max(self.peak_bytes, self._in_use)
-                        self._in_flight += 1
+                        group = [self._queue.popleft()]
+                        key = self._group_key(head)
+                        taken = head.need
+                        rest = collections.deque()
+                        while self._queue and len(group) < self.max_group:
+                            r = self._queue.popleft()
+                            if self._group_key(r) == key and self._in_use + taken + r.need <= self.budget:
+                                group.append(r)
+                                taken += r.need
+                            else:
+                                rest.append(r)
+                        rest.extend(self._queue)
+                        self._queue = rest
+                        self._in_use += taken
+                        self._in_flight += len(group)
                         self.peak_in_flight = max(self.peak_in_flight, self._in_flight)
-                        return head
+                        self.peak_bytes = max(self.peak_bytes, self._in_use)
+                        return group
                 elif self._closed:
                     return None
                 self._cv.wait()
 
-    def _release(self, req: _Request):
+    def _release(self, group: List[_Request]):
         with self._cv:
-            self._in_use -= req.need
-            self._in_flight -= 1
+            for req in group:
+                self._in_use -= req.need
+            self._in_flight -= len(group)
             self._cv.notify_all()
 
     def _work(self, slot: int):
@@ -279,24 +371,34 @@ class DecryptionServer:
         torch.cuda.set_device(self.device)
         stream = torch.cuda.Stream(device=self.device)
         while True:
-            req = self._admit()
-            if req is None:
+            group = self._admit()
+            if group is None:
                 return
-            req.started = time.perf_counter()
+            now = time.perf_counter()
+            for req in group:
+                req.started = now
             try:
+                rng = ChaCha20Rng.seed_from_u64(group[0].seed)
                 with torch.cuda.stream(stream):
-                    out = decrypt_request(self.dk, req.ciphertexts, req.party_keys,
-                                          ChaCha20Rng.seed_from_u64(req.seed), self.cache)
+                    if len(group) == 1:
+                        outs = [decrypt_request(self.dk, group[0].ciphertexts, group[0].party_keys, rng, self.cache)]
+                    else:
+                        outs = decrypt_group(self.dk, [r.ciphertexts for r in group], group[0].party_keys, rng,
+                                             self.cache)
                 stream.synchronize()
                 done = time.perf_counter()
                 with self._cv:
-                    self.latencies.append(done - req.submitted)
-                    self.completed_ciphertexts += len(req.ciphertexts)
-                req.future.set_result(out)
-            except BaseException as exc:  # noqa: BLE001 -- reported through the future
-                req.future.set_exception(exc)
+                    for req in group:
+                        self.latencies.append(done - req.submitted)
+                        self.completed_ciphertexts += len(req.ciphertexts)
+                for req, out in zip(group, outs):
+                    req.future.set_result(out)
+            except BaseException as exc:  # noqa: BLE001 -- reported through the futures
+                for req in group:
+                    if not req.future.done():
+                        req.future.set_exception(exc)
             finally:
-                self._release(req)
+                self._release(group)
 
 
 def run_concurrent(fn: Callable, items: Sequence, slots: int):

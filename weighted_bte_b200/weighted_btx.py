@@ -704,6 +704,53 @@ def validate_batch(decryption_key: PublicDecryptionKey, ciphertexts: Sequence[Ci
                           valid, first, first_dev, valid_dev)
 
 
+def validate_batches(decryption_key: PublicDecryptionKey, batches: Sequence) -> List[ValidatedBatch]:
+    """`validate_batch` for several batches with one compression pass and one
+    proof-check launch over all their ciphertexts; each result equals
+    `validate_batch` of that batch alone."""
+    if not batches:
+        return []
+    for cts in batches:
+        _validate_batch_size(decryption_key, len(cts))
+    sizes = [len(cts) for cts in batches]
+    total = sum(sizes)
+    torch = _t()
+
+    def dev(cts, attr, rec):
+        if isinstance(cts, CiphertextBatch):
+            return getattr(cts, attr)[: rec * len(cts)]
+        if attr == "first":
+            return to_device(b"".join(c.first for c in cts))
+        if attr == "commitment":
+            return to_device(b"".join(c.proof.commitment for c in cts))
+        return to_device(b"".join(c.second for c in cts))
+
+    first_all = torch.cat([dev(cts, "first", G1B) for cts in batches])
+    comm_all = torch.cat([dev(cts, "commitment", G1B) for cts in batches])
+    second_all = torch.cat([dev(cts, "second", GTB) for cts in batches])
+    first_c = ops.split(ops.g1_compress(first_all, total), 48)
+    comm_c = ops.split(ops.g1_compress(comm_all, total), 48)
+    second_enc = append_gt_many(second_all, total)
+    responses = [r for cts in batches for r in _responses(cts)]
+    cs = _challenges(decryption_key.setup_id(), first_c, second_enc, comm_c)
+    ok = np.zeros(total, dtype=np.uint8)
+    ops.ctx().call("wbte_schnorr_verify", ok, first_all, comm_all, ops.scalars_bytes(responses), ops.scalars_bytes(cs),
+                   total)
+    valid_all = ok.astype(bool)
+    valid_dev_all = to_device(ok.tobytes())
+    first_masked = (first_all.view(total, G1B) * valid_dev_all[:total].view(total, 1)).reshape(-1)
+    out, o = [], 0
+    for cts, n in zip(batches, sizes):
+        enc = (None, None, first_c[o : o + n], comm_c[o : o + n], second_enc[o : o + n])
+        if isinstance(cts, CiphertextBatch) and cts._digest is None:
+            cts._enc = (cts.first, cts.commitment) + enc[2:]
+        digest = batch_digest(cts, enc)
+        out.append(ValidatedBatch(decryption_key.setup_id(), n, digest, valid_all[o : o + n], None,
+                                  first_masked[G1B * o : G1B * (o + n)], valid_dev_all[o : o + n]))
+        o += n
+    return out
+
+
 def partial_decrypt_many(party_keys: Sequence[PartySecretKey], batch: ValidatedBatch) -> List[DecryptionShare]:
     """`partial_decrypt` for several parties in one launch sequence
     (weighted_btx/src/decryption.rs:205-233)."""
@@ -749,9 +796,9 @@ def verify_decryption_share(decryption_key: PublicDecryptionKey, batch: Validate
     return _verify_shares(decryption_key, batch, [share], [1])
 
 
-def accept_decryption_shares(decryption_key: PublicDecryptionKey, batch: ValidatedBatch,
-                             shares: Sequence[DecryptionShare], rng=None) -> AcceptedDecryptionShares:
-    """weighted_btx/src/decryption.rs:276-353 (batched check, per-share fallback, weight check)."""
+def screen_shares(decryption_key: PublicDecryptionKey, batch: ValidatedBatch, shares: Sequence[DecryptionShare]):
+    """The structural checks of accept_decryption_shares (weighted_btx/src/decryption.rs:282-305):
+    returns (candidates bound to this batch and setup, rejected party indices)."""
     _validate_batch_size(decryption_key, batch.batch_size())
     if batch.setup_id() != decryption_key.setup_id():
         raise E.MismatchedSetup()
@@ -769,14 +816,16 @@ def accept_decryption_shares(decryption_key: PublicDecryptionKey, batch: Validat
             candidates.append(s)
         else:
             rejected.append(s.party_index)
-    rng = rng or OsRng()
-    if candidates:
-        challenges = [sample_nonzero(rng) for _ in candidates]
-        aggregate_ok = _verify_shares(decryption_key, batch, candidates, challenges)
-    else:
-        aggregate_ok = True
+    return candidates, rejected
+
+
+def finish_acceptance(decryption_key: PublicDecryptionKey, batch: ValidatedBatch, candidates, rejected,
+                      aggregate_ok: bool) -> AcceptedDecryptionShares:
+    """The rest of accept_decryption_shares (decryption.rs:306-353) once the
+    batched aggregate check has run: per-share blame on failure, weight check."""
+    rejected = list(rejected)
     if aggregate_ok:
-        accepted = candidates
+        accepted = list(candidates)
     else:
         accepted = []
         for s in candidates:
@@ -791,6 +840,19 @@ def accept_decryption_shares(decryption_key: PublicDecryptionKey, batch: Validat
         raise E.InsufficientWeight(weight, decryption_key.required_weight(), rejected)
     return AcceptedDecryptionShares(decryption_key.setup_id(), batch.batch_size(), batch.digest(), weight, accepted,
                                     rejected)
+
+
+def accept_decryption_shares(decryption_key: PublicDecryptionKey, batch: ValidatedBatch,
+                             shares: Sequence[DecryptionShare], rng=None) -> AcceptedDecryptionShares:
+    """weighted_btx/src/decryption.rs:276-353 (batched check, per-share fallback, weight check)."""
+    candidates, rejected = screen_shares(decryption_key, batch, shares)
+    rng = rng or OsRng()
+    if candidates:
+        challenges = [sample_nonzero(rng) for _ in candidates]
+        aggregate_ok = _verify_shares(decryption_key, batch, candidates, challenges)
+    else:
+        aggregate_ok = True
+    return finish_acceptance(decryption_key, batch, candidates, rejected, aggregate_ok)
 
 
 def transform_size_for(batch_size: int) -> int:
