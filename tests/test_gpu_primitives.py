@@ -144,7 +144,7 @@ def test_group_ntt_matches_oracle(orc, n):
         assert ops.split(ops.g2_ntt(b"".join(g2), inverse=inv), 192) == orc.g2_ntt(g2, inverse=inv)
 
 
-@pytest.mark.parametrize("n", [2, 16])
+@pytest.mark.parametrize("n", [2, 4, 8, 16, 32])
 def test_gt_transforms_match_oracle(orc, n):
     rng = random.Random(400 + n)
     e = orc.pairing(orc.g1_generator(), orc.g2_generator())

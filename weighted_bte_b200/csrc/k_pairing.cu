@@ -152,6 +152,71 @@ __global__ void __launch_bounds__(WARP) k_gt_stage(uint8_t* io, const uint8_t* t
     }
 }
 
+// x^(omega_4) under the decomposed action.  The forward domain's primitive
+// 4th root of unity is omega_4 = |x|^3 (its base-|x| digits are 0, 0, 0, 1),
+// which acts as conj(Frobenius^3(x)); the inverse domain's omega_4^-1 acts as
+// its inverse, Frobenius^3(x).  (Agrees with the plain power after the hard
+// part, like every decomposed action.)
+WBTE_INL void gt_omega4(Fp12& r, const Fp12& x, bool inverse) {
+    fp12_frobenius(r, x, 3);
+    if (!inverse) fp12_conj(r, r);
+}
+
+// One radix-4 DIT stage merging the radix-2 stages of half sizes h and 2h:
+// per block of 4h and offset j < h, with a, b, c, d at j, j+h, j+2h, j+3h and
+// w1 = w^(2j s), w2 = w^(j s), w3 = w1 w2 (s = n / 4h):
+//   t1 = b^w1, u = c^w2, v = d^w3, cw = u v, dw = (u / v)^omega_4
+//   j: a t1 cw   j+h: a/t1 dw   j+2h: a t1 / cw   j+3h: a/t1 / dw
+// Three exponentiations per four outputs instead of the radix-2 pair's four.
+// Each exponentiation is split over the group's 4 lanes (one base-|x| digit
+// each) and combined in shared memory.  prefix: write only the first two
+// outputs (the last stage of the truncated inverse transform).
+__global__ void __launch_bounds__(WARP) k_gt_radix4(uint8_t* io, const uint8_t* tw, int64_t n, int64_t h,
+                                                   int64_t count, int inverse, int prefix) {
+    __shared__ Fp12 sh[WARP];
+    const int lane = threadIdx.x, c = lane % GT_LANES;
+    const int64_t t = ((int64_t)blockIdx.x * WARP + lane) / GT_LANES;
+    const bool active = t < (n / 4) * count;
+    const int64_t q = active ? t / (n / 4) : 0, tt = active ? t % (n / 4) : 0;
+    const int64_t blk = tt / h, j = tt % h;
+    Fp12* base = as_gt(io) + q * n + blk * 4 * h + j;
+    const int64_t s = n / (4 * h);
+    Fp12 a, ex[3];
+    if (active) a = load_vec(base);  // read before any output of the group is written
+    for (int e = 0; e < 3; e++) {
+        int64_t idx = (e == 0 ? 2 * j : (e == 1 ? j : 3 * j)) * s;
+        const bool neg = idx >= n / 2;  // w^(k + n/2) = -w^k: the inverse
+        if (neg) idx -= n / 2;
+        Fp12 part = fp12_one();
+        if (active) {
+            Fp12 x = load_vec(base + (int64_t)(e + 1) * h);
+            if (idx != 0) gt_pow_part(part, x, tw + FR_SZ * idx, c);
+            else if (c == 0) part = x;
+        }
+        __syncwarp();  // the previous exponentiation's result has been read
+        store_vec(sh + lane, part);
+        gt_combine(sh, lane, c);
+        ex[e] = load_vec(sh + (lane - c));
+        if (neg) fp12_conj(ex[e], ex[e]);
+    }
+    if (!active || (prefix && c >= 2)) return;
+    Fp12 r, m;
+    if (c == 0 || c == 2) {
+        fp12_mul(m, ex[1], ex[2]);  // cw
+    } else {
+        fp12_conj(m, ex[2]);
+        fp12_mul(m, ex[1], m);
+        gt_omega4(m, m, inverse != 0);  // dw
+    }
+    if (c >= 2) fp12_conj(m, m);
+    Fp12 t1 = ex[0];
+    if (c & 1) fp12_conj(t1, t1);
+    fp12_mul(r, a, t1);
+    fp12_mul(r, r, m);
+    const int64_t pos = c == 0 ? 0 : (c == 1 ? h : (c == 2 ? 2 * h : 3 * h));
+    store_vec(base + pos, r);
+}
+
 // last stage keeping only the first out_count outputs
 __global__ void __launch_bounds__(WARP) k_gt_last_prefix(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count,
                                                         int64_t count) {
@@ -303,7 +368,7 @@ void launch_final_exp(uint8_t* out, const uint8_t* in, int64_t n, FinalExpMode m
 }
 
 static void gt_transform(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count, bool prefix, cudaStream_t s,
-                         int64_t count) {
+                         int64_t count, bool inverse) {
     ProfScope prof_("gt_ifft", s);
     if (n <= 1 || count <= 0) return;
     int bits = 0;
@@ -312,24 +377,42 @@ static void gt_transform(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_
     if (cudaMallocAsync(&tmp, GT_SZ * (size_t)(n * count), s) != cudaSuccess) return;
     note_launch();
     k_gt_bitrev<<<blocks_for(n * count), TPB, 0, s>>>(tmp, io, n, bits, count);
-    int64_t last_half = prefix ? n / 4 : n / 2;
-    for (int64_t half = 1; half <= last_half; half *= 2) {
-        note_launch();
-        k_gt_stage<<<blocks_for(GT_LANES * (n / 2) * count, WARP), WARP, 0, s>>>(tmp, tw, n, half, count);
-    }
-    if (prefix && out_count > 0) {
-        note_launch();
-        k_gt_last_prefix<<<blocks_for(GT_LANES * out_count * count, WARP), WARP, 0, s>>>(tmp, tw, n, out_count, count);
+    if (n < 4 || (prefix && out_count != n / 2)) {
+        // radix-2 throughout (tiny transforms, or a prefix other than the first half)
+        int64_t last_half = prefix ? n / 4 : n / 2;
+        for (int64_t half = 1; half <= last_half; half *= 2) {
+            note_launch();
+            k_gt_stage<<<blocks_for(GT_LANES * (n / 2) * count, WARP), WARP, 0, s>>>(tmp, tw, n, half, count);
+        }
+        if (prefix && out_count > 0) {
+            note_launch();
+            k_gt_last_prefix<<<blocks_for(GT_LANES * out_count * count, WARP), WARP, 0, s>>>(tmp, tw, n, out_count,
+                                                                                             count);
+        }
+    } else {
+        // an odd number of stages starts with one radix-2 stage, the rest pair up
+        int64_t half = 1;
+        if (bits & 1) {
+            note_launch();
+            k_gt_stage<<<blocks_for(GT_LANES * (n / 2) * count, WARP), WARP, 0, s>>>(tmp, tw, n, 1, count);
+            half = 2;
+        }
+        for (; half < n; half *= 4) {
+            const bool last = 4 * half == n;
+            note_launch();
+            k_gt_radix4<<<blocks_for(GT_LANES * (n / 4) * count, WARP), WARP, 0, s>>>(
+                tmp, tw, n, half, count, inverse ? 1 : 0, (prefix && last) ? 1 : 0);
+        }
     }
     cudaMemcpyAsync(io, tmp, GT_SZ * (size_t)(n * count), cudaMemcpyDeviceToDevice, s);
     cudaFreeAsync(tmp, s);
 }
 void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* tw_inv, int64_t n, int64_t out_count, cudaStream_t s,
                                    int64_t count) {
-    gt_transform(io, tw_inv, n, out_count, true, s, count);
+    gt_transform(io, tw_inv, n, out_count, true, s, count, true);
 }
-void launch_gt_ntt(uint8_t* io, const uint8_t* tw, int64_t n, cudaStream_t s, int64_t count) {
-    gt_transform(io, tw, n, n, false, s, count);
+void launch_gt_ntt(uint8_t* io, const uint8_t* tw, int64_t n, cudaStream_t s, int64_t count, bool inverse) {
+    gt_transform(io, tw, n, n, false, s, count, inverse);
 }
 
 void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint8_t* scalars, int64_t n, cudaStream_t s) {

@@ -118,7 +118,8 @@ void launch_final_exp(uint8_t* out, const uint8_t* in, int64_t n, FinalExpMode m
 void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* twiddles_inv, int64_t n, int64_t out_count, cudaStream_t s,
                                    int64_t count = 1);
 // full unscaled transform over GT values (forward if twiddles are powers of w, inverse with w^-1)
-void launch_gt_ntt(uint8_t* io, const uint8_t* twiddles, int64_t n, cudaStream_t s, int64_t count = 1);
+// twiddles from the inverse domain when inverse is set (selects the omega_4 action)
+void launch_gt_ntt(uint8_t* io, const uint8_t* twiddles, int64_t n, cudaStream_t s, int64_t count = 1, bool inverse = false);
 // out[i] = base[i * stride]^scalars[i] on GT
 void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t base_stride, const uint8_t* scalars, int64_t n, cudaStream_t s);
 // out[i] = a[i * sa] * b[i * sb] (conj_b: b conjugated)

@@ -211,6 +211,31 @@ void fp12_product(Call& c, uint8_t* out, const uint8_t* in, int64_t n) {
     }
 }
 
+// out[b] = product of in[b len .. (b + 1) len) for b < K, by levels of
+// products of 16 so that long segments spread over many threads
+void fp12_segments_product(Call& c, uint8_t* out, const uint8_t* in, int64_t len, int64_t K) {
+    if (len <= 0 || K <= 0) return;
+    const int64_t G = 16;
+    const uint8_t* cur = in;
+    while (true) {
+        int64_t groups = (len + G - 1) / G;
+        // group j of segment b spans [b len + j G, next group's start); the last
+        // group of a segment ends where the next segment begins, so no group
+        // crosses a segment boundary
+        std::vector<int64_t> offs(K * groups + 1);
+        for (int64_t b = 0; b < K; b++)
+            for (int64_t j = 0; j < groups; j++) offs[b * groups + j] = b * len + j * G;
+        offs[K * groups] = K * len;
+        uint8_t* dst = groups == 1 ? out : c.alloc(GT_SZ * K * groups);
+        const int64_t* doffs = c.in_vec(offs);
+        if (!c.ok()) return;
+        launch_fp12_segment_product(dst, cur, doffs, K * groups, c.s);
+        if (groups == 1) return;
+        cur = dst;
+        len = groups;
+    }
+}
+
 // G2 generator affine bytes on the device
 uint8_t* g2_generator_dev(Call& c) {
     uint8_t one[32] = {1};
@@ -507,7 +532,7 @@ int32_t wbte_gt_ntt(wbte_ctx* ctx, void* io, uint64_t n, int32_t inverse) {
     if (n == 1) return c.finish();
     uint8_t* d = c.inout(io, GT_SZ * n);
     const uint8_t* tw = twiddles(c, (int64_t)n, inverse != 0);
-    if (c.ok()) launch_gt_ntt(d, tw, (int64_t)n, c.s);
+    if (c.ok()) launch_gt_ntt(d, tw, (int64_t)n, c.s, 1, inverse != 0);
     return c.finish();
 }
 
@@ -1299,7 +1324,7 @@ int32_t wbte_wpfe_precompute(wbte_ctx* ctx, void* first_cauchy, void* pairing_ca
     launch_gt_pow(h, f, 1, dcoef, (int64_t)B, c.s);
     launch_gather(f, h, drot, (int64_t)B, GT_SZ, c.s);
     launch_fp12_conj(f, f, (int64_t)B, c.s);
-    if (B > 1) launch_gt_ntt(f, twi, (int64_t)B, c.s);
+    if (B > 1) launch_gt_ntt(f, twi, (int64_t)B, c.s, 1, true);
     cudaMemcpyAsync(dpc, f, GT_SZ * B, cudaMemcpyDeviceToDevice, c.s);
     return c.finish();
 }
@@ -1403,7 +1428,7 @@ static void pfe_conv_gt(Call& c, uint8_t* io, const uint8_t* E, const uint8_t* c
     launch_gather(h, a, rot, (int64_t)B, GT_SZ, c.s);
     launch_gt_pow(b, h, 1, cvec, (int64_t)B, c.s);
     launch_fp12_mul(io, b, 1, a, 1, true, (int64_t)B, c.s);
-    if (B > 1) launch_gt_ntt(io, twi, (int64_t)B, c.s);
+    if (B > 1) launch_gt_ntt(io, twi, (int64_t)B, c.s, 1, true);
 }
 
 struct PfeConvTables {
@@ -1623,7 +1648,7 @@ int32_t wbte_wbtx_verify_shares_many(wbte_ctx* ctx, int32_t* ok, const wbte_wbtx
     uint8_t* f = c.alloc(GT_SZ * P1 * K);
     uint8_t* prod = c.alloc(GT_SZ * K);
     uint8_t* flags = c.alloc(K);
-    std::vector<int64_t> sbase(K), vbase(B * K), offs(K + 1);
+    std::vector<int64_t> sbase(K), vbase(B * K);
     std::vector<int32_t> svsel(K), vvsel(B * K), gidx(K, 0);
     for (uint64_t b = 0; b < K; b++) {
         sbase[b] = (int64_t)(b * T);
@@ -1633,14 +1658,12 @@ int32_t wbte_wbtx_verify_shares_many(wbte_ctx* ctx, int32_t* ok, const wbte_wbtx
             vvsel[b * B + i] = (int32_t)b;
         }
     }
-    for (uint64_t b = 0; b <= K; b++) offs[b] = (int64_t)(b * P1);
     const int64_t* dsbase = c.in_vec(sbase);
     const int32_t* dsvsel = c.in_vec(svsel);
     const int64_t* dvbase = c.in_vec(vbase);
     const int32_t* dvvsel = c.in_vec(vvsel);
     const int32_t* dpidx = c.in_vec(pidx);
     const int32_t* dgidx = c.in_vec(gidx);
-    const int64_t* doffs = c.in_vec(offs);
     uint8_t* g2 = g2_generator_dev(c);
     if (!c.ok()) return c.finish();
     launch_msm_family(GROUP_G1, agg, dsig, dsbase, nullptr, dch, dsvsel, (int32_t)K, (int64_t)K, (int64_t)T, c.s);
@@ -1654,7 +1677,7 @@ int32_t wbte_wbtx_verify_shares_many(wbte_ctx* ctx, int32_t* ok, const wbte_wbtx
     launch_gather(gcol, g2, dgidx, (int64_t)K, G2_AFF, c.s);
     cudaMemcpy2DAsync(Q + G2_AFF * B, G2_AFF * P1, gcol, G2_AFF, G2_AFF, K, cudaMemcpyDeviceToDevice, c.s);
     launch_miller(f, P, Q, (int64_t)(P1 * K), c.s);
-    launch_fp12_segment_product(prod, f, doffs, (int64_t)K, c.s);
+    fp12_segments_product(c, prod, f, (int64_t)P1, (int64_t)K);
     launch_final_exp(prod, prod, (int64_t)K, FE_FULL, c.s);
     launch_fp12_is_one(flags, prod, (int64_t)K, c.s);
     std::vector<uint8_t> h(K);
