@@ -124,7 +124,30 @@ static void mont_mul_n(u64 *out, const u64 *a, const u64 *b, const u64 *m, u64 m
 /* ------------------------------------------------------------------ */
 /* Fp                                                                 */
 /* ------------------------------------------------------------------ */
-static inline void fp_mul(fp *o, const fp *a, const fp *b) { mont_mul_n(o->l, a->l, b->l, P_L, P_INV, 6); }
+/* Work counting (built only into the counting library, single-threaded, see
+ * the Makefile): every Fp Montgomery product or square counts once. */
+#ifdef ORC_COUNT_MULS
+static unsigned long long g_fp_products;
+#define ORC_COUNT_FP() (g_fp_products++)
+#else
+#define ORC_COUNT_FP() ((void)0)
+#endif
+unsigned long long orc_fp_product_count(void) {
+#ifdef ORC_COUNT_MULS
+    return g_fp_products;
+#else
+    return 0;
+#endif
+}
+void orc_fp_product_count_reset(void) {
+#ifdef ORC_COUNT_MULS
+    g_fp_products = 0;
+#endif
+}
+static inline void fp_mul(fp *o, const fp *a, const fp *b) {
+    ORC_COUNT_FP();
+    mont_mul_n(o->l, a->l, b->l, P_L, P_INV, 6);
+}
 static inline void fp_sqr(fp *o, const fp *a) { fp_mul(o, a, a); }
 static inline void fp_add(fp *o, const fp *a, const fp *b) {
     u64 c = add_n(o->l, a->l, b->l, 6);

@@ -194,3 +194,28 @@ def test_chacha20_block_matches_rfc8439():
     key = list(struct.unpack("<8I", bytes(range(32))))
     out = chacha20_block(key, 1 | (0x09000000 << 32), 0x4A000000)
     assert out[0] == 0xE4E7F110 and out[1] == 0x15593BD1 and out[15] == 0x4E3C50A2
+
+
+def test_work_counts_reproduce(orc):
+    """The counting build of the oracle reproduces the recorded work table
+    (oracle/count_work.py) for the hard final exponentiation, and counts
+    nothing in the regular build."""
+    import ctypes
+    import json
+    import os
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    count = ctypes.CDLL(os.path.join(root, "oracle", "_build", "liboracle_count.so"))
+    count.orc_init()
+    count.orc_fp_product_count.restype = ctypes.c_ulonglong
+    with open(os.path.join(root, "weighted_bte_b200", "algorithmic_work.json")) as f:
+        table = json.load(f)
+    f12 = orc.easy_final_exp(orc.miller_loop(orc.g1_generator(), orc.g2_generator()))
+    out = ctypes.create_string_buffer(576)
+    count.orc_fp_product_count_reset()
+    count.orc_hard_final_exp(out, f12)
+    assert count.orc_fp_product_count() == table["hard_final_exp"]["fp_products"]
+    assert out.raw == orc.hard_final_exp(f12)
+    plain = orc.lib()
+    plain.orc_fp_product_count.restype = ctypes.c_ulonglong
+    assert plain.orc_fp_product_count() == 0
