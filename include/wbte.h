@@ -239,6 +239,9 @@ int32_t wbte_wbtx_open(wbte_ctx *ctx, void *messages, const void *opening_keys, 
  *                         challenges K*T Fr, party_indices T (host)
  *   precompute_many       beta K*B GT over the committee's kernel lines
  *   open_many             messages K*B GT, opening_keys B*T G2 (shared),
+ *                         opening_lines: their line tables (wbte_g2_prepare_lines
+ *                         of the B*T keys) or NULL; with them each slot's T
+ *                         pairings share one multi-Miller loop (T <= 8),
  *                         sigma K*T G1, second/beta K*B GT, valid K*B. */
 int32_t wbte_wbtx_partial_decrypt_many(wbte_ctx *ctx, void *sigma, const void *first, uint64_t batch_size,
                                        const void *q, uint64_t T, uint64_t K);
@@ -247,9 +250,9 @@ int32_t wbte_wbtx_verify_shares_many(wbte_ctx *ctx, int32_t *ok, const wbte_wbtx
                                      const void *challenges, uint64_t T, uint64_t K);
 int32_t wbte_wbtx_precompute_many(wbte_ctx *ctx, void *beta, const void *kernel_lines, const void *first,
                                   const uint8_t *valid, uint64_t batch_size, uint64_t K);
-int32_t wbte_wbtx_open_many(wbte_ctx *ctx, void *messages, const void *opening_keys, const void *sigma, uint64_t T,
-                            const void *second, const void *beta, const uint8_t *valid, uint64_t batch_size,
-                            uint64_t K);
+int32_t wbte_wbtx_open_many(wbte_ctx *ctx, void *messages, const void *opening_keys, const void *opening_lines,
+                            const void *sigma, uint64_t T, const void *second, const void *beta,
+                            const uint8_t *valid, uint64_t batch_size, uint64_t K);
 /* Public key material of keygen_with_rng (weighted_btx/src/setup.rs:98-233):
  *   verification_keys[i * N + j] = [q_pos[i * N + j]] G2            (i < L)
  *   negative[i * W + w]          = [z[w] q_neg[i * N + owner[w]]] G2 (i < L)

@@ -42,6 +42,20 @@ __global__ void k_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t
     store_vec(as_gt(out) + i, f);
 }
 
+// out[o] = prod_{t < T} Miller(P[(o / per) * T + t], lines of table (o % per) * T + t):
+// the opening of K batches against one committee's prepared opening keys
+// (tables line-major with stride per * T), each batch with its own T shares.
+__global__ void k_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per,
+                                     int T) {
+    int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const int64_t b = o / per, i = o % per;
+    Fp12 f;
+    multi_miller_loop_lines(f, reinterpret_cast<const Line*>(lines) + i * T, (size_t)(per * T), 1,
+                            reinterpret_cast<const G1A*>(p) + b * T, T);
+    store_vec(as_gt(out) + o, f);
+}
+
 __global__ void k_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, int64_t p_mod, int64_t q_mod) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -94,6 +108,10 @@ __global__ void k_gt_bitrev(uint8_t* dst, const uint8_t* src, int64_t n, int bit
 // (gt_pow_lane); the four parts meet in shared memory.  Blocks are one warp.
 constexpr int GT_LANES = 4;
 constexpr int WARP = 32;
+// resident blocks per SM the GT kernels are compiled for (register budget)
+#ifndef WBTE_GT_MINBLOCKS
+#define WBTE_GT_MINBLOCKS 1
+#endif
 
 // parts of v^s for the butterfly or element this lane belongs to
 WBTE_INL void gt_pow_part(Fp12& part, const Fp12& v, const uint8_t* scalar, int c) {
@@ -123,7 +141,7 @@ WBTE_INL void gt_combine(Fp12* sh, int lane, int c) {
 
 // One butterfly per group of lanes: u' = u t, v' = u t^-1 with t = v^tw
 // (inverse by conjugation in the cyclotomic subgroup).
-__global__ void __launch_bounds__(WARP) k_gt_stage(uint8_t* io, const uint8_t* tw, int64_t n, int64_t half,
+__global__ void __launch_bounds__(WARP, WBTE_GT_MINBLOCKS) k_gt_stage(uint8_t* io, const uint8_t* tw, int64_t n, int64_t half,
                                                   int64_t count) {
     __shared__ Fp12 sh[WARP];
     const int lane = threadIdx.x, c = lane % GT_LANES;
@@ -171,7 +189,7 @@ WBTE_INL void gt_omega4(Fp12& r, const Fp12& x, bool inverse) {
 // Each exponentiation is split over the group's 4 lanes (one base-|x| digit
 // each) and combined in shared memory.  prefix: write only the first two
 // outputs (the last stage of the truncated inverse transform).
-__global__ void __launch_bounds__(WARP) k_gt_radix4(uint8_t* io, const uint8_t* tw, int64_t n, int64_t h,
+__global__ void __launch_bounds__(WARP, WBTE_GT_MINBLOCKS) k_gt_radix4(uint8_t* io, const uint8_t* tw, int64_t n, int64_t h,
                                                    int64_t count, int inverse, int prefix) {
     __shared__ Fp12 sh[WARP];
     const int lane = threadIdx.x, c = lane % GT_LANES;
@@ -218,7 +236,7 @@ __global__ void __launch_bounds__(WARP) k_gt_radix4(uint8_t* io, const uint8_t* 
 }
 
 // last stage keeping only the first out_count outputs
-__global__ void __launch_bounds__(WARP) k_gt_last_prefix(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count,
+__global__ void __launch_bounds__(WARP, WBTE_GT_MINBLOCKS) k_gt_last_prefix(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count,
                                                         int64_t count) {
     __shared__ Fp12 sh[WARP];
     const int lane = threadIdx.x, c = lane % GT_LANES;
@@ -242,7 +260,7 @@ __global__ void __launch_bounds__(WARP) k_gt_last_prefix(uint8_t* io, const uint
     }
 }
 
-__global__ void __launch_bounds__(WARP) k_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint8_t* scalars, int64_t n) {
+__global__ void __launch_bounds__(WARP, WBTE_GT_MINBLOCKS) k_gt_pow(uint8_t* out, const uint8_t* base, int64_t stride, const uint8_t* scalars, int64_t n) {
     __shared__ Fp12 sh[WARP];
     const int lane = threadIdx.x, c = lane % GT_LANES;
     const int64_t i = ((int64_t)blockIdx.x * WARP + lane) / GT_LANES;
@@ -348,6 +366,15 @@ void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, 
     if (n <= 0) return;
     note_launch();
     k_miller<<<blocks_for(n), TPB, 0, s>>>(out, p, q, n, p_mod, q_mod);
+}
+bool launch_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per, int T,
+                               cudaStream_t s) {
+    ProfScope prof_("miller_lines_multi", s);
+    if (T < 1 || T > MULTI_MILLER_MAX) return false;
+    if (n <= 0) return true;
+    note_launch();
+    k_miller_lines_multi<<<blocks_for(n), TPB, 0, s>>>(out, lines, p, n, per, T);
+    return true;
 }
 void launch_fp12_mask(uint8_t* io, const uint8_t* valid, int64_t n, cudaStream_t s) {
     if (n <= 0) return;

@@ -102,6 +102,11 @@ void launch_msm_family_scratch(Group g, uint8_t* out, const uint8_t* points, con
 // lines[step * n + i] for step < 68: prepared line coefficients of q[i]
 void launch_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n, cudaStream_t s);
 // out[i] = Miller(p[i], lines of pair i), lines laid out as above with n pairs
+// out[o] = prod_{t<T} Miller(p[(o / per) T + t], line table (o % per) T + t) for o < n
+// (tables line-major, stride per * T); returns false when T exceeds the
+// supported pair count (8), launching nothing.
+bool launch_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per, int T,
+                               cudaStream_t s);
 void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, cudaStream_t s,
                          int64_t lines_n = 0);
 // out[i] = Miller(p[p_mod ? i % p_mod : i], q[i])

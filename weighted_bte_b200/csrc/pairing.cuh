@@ -103,6 +103,38 @@ static __device__ __noinline__ void miller_loop_lines(Fp12& f, const Line* lines
     fp12_conj(f, f);
 }
 
+// Product of T <= MULTI_MILLER_MAX Miller loops over precomputed lines
+// sharing one accumulator, so the 62 Fp12 squarings are paid once for all T
+// pairs.  Pair t uses the G1 point at points[t] (device memory) and the line
+// table at lines + t * pair_stride (lines of one table `stride` apart);
+// identities contribute 1.
+constexpr int MULTI_MILLER_MAX = 8;
+static __device__ __noinline__ void multi_miller_loop_lines(Fp12& f, const Line* lines, size_t stride,
+                                                            size_t pair_stride, const G1A* points, int T) {
+    G1A P[MULTI_MILLER_MAX];
+    for (int t = 0; t < T; t++) P[t] = load_affine(points + t);
+    f = fp12_one();
+    int idx = 0;
+    for (int i = 62; i >= 0; i--) {
+        if (i != 62) fp12_sqr(f, f);
+        for (int t = 0; t < T; t++) {
+            if (is_inf(P[t])) continue;
+            Line l = load_vec(lines + t * pair_stride + stride * idx);
+            mul_by_line(f, l, P[t]);
+        }
+        idx++;
+        if ((X_ABS >> i) & 1) {
+            for (int t = 0; t < T; t++) {
+                if (is_inf(P[t])) continue;
+                Line l = load_vec(lines + t * pair_stride + stride * idx);
+                mul_by_line(f, l, P[t]);
+            }
+            idx++;
+        }
+    }
+    fp12_conj(f, f);
+}
+
 // ------------------------------------------------- final exponentiation
 // f^((p^6 - 1)(p^2 + 1))
 static __device__ __noinline__ void final_exp_easy(Fp12& r, const Fp12& f) {

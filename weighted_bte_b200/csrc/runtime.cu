@@ -1717,8 +1717,9 @@ int32_t wbte_wbtx_precompute_many(wbte_ctx* ctx, void* beta, const void* kernel_
     return c.finish();
 }
 
-int32_t wbte_wbtx_open_many(wbte_ctx* ctx, void* messages, const void* opening_keys, const void* sigma, uint64_t T,
-                            const void* second, const void* beta, const uint8_t* valid, uint64_t B, uint64_t K) {
+int32_t wbte_wbtx_open_many(wbte_ctx* ctx, void* messages, const void* opening_keys, const void* opening_lines,
+                            const void* sigma, uint64_t T, const void* second, const void* beta, const uint8_t* valid,
+                            uint64_t B, uint64_t K) {
     if (!ctx) return WBTE_ERR_INVALID_ARG;
     Call c(ctx);
     if (!messages || !opening_keys || !sigma || !second || !beta || !valid || B == 0 || T == 0 || K == 0)
@@ -1730,9 +1731,19 @@ int32_t wbte_wbtx_open_many(wbte_ctx* ctx, void* messages, const void* opening_k
     const uint8_t* db = c.in(beta, GT_SZ * B * K);
     const uint8_t* dv = c.in(valid, B * K);
     const uint64_t BT = B * T;
+    uint8_t* alpha = c.alloc(GT_SZ * B * K);
+    if (opening_lines && T <= 8) {
+        // prepared opening keys: one multi-Miller loop per slot shares the
+        // squarings across the T shares
+        const uint8_t* dl = c.in(opening_lines, LINE_SZ * LINES_PER_POINT * BT);
+        if (!c.ok()) return c.finish();
+        launch_miller_lines_multi(alpha, dl, ds, (int64_t)(B * K), (int64_t)B, (int)T, c.s);
+        launch_final_exp(alpha, alpha, (int64_t)(B * K), FE_FULL, c.s);
+        launch_unmask(dm, d2, alpha, db, dv, (int64_t)(B * K), c.s);
+        return c.finish();
+    }
     uint8_t* P = c.alloc(G1_AFF * BT * K);
     uint8_t* f = c.alloc(GT_SZ * BT * K);
-    uint8_t* alpha = c.alloc(GT_SZ * B * K);
     std::vector<int32_t> pidx(BT * K);
     for (uint64_t b = 0; b < K; b++)
         for (uint64_t x = 0; x < BT; x++) pidx[b * BT + x] = (int32_t)(b * T + x % T);

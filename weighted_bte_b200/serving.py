@@ -120,7 +120,7 @@ class CommitteeCache:
                 ev.record(torch.cuda.current_stream())
                 entry.ready = ev
                 entry.nbytes = sum(t.numel() for t in (entry.pre.kernel_lines, entry.pre.opening_keys,
-                                                        entry.pre.transformed_kernel))
+                                                        entry.pre.opening_lines, entry.pre.transformed_kernel))
             except BaseException as exc:  # noqa: BLE001 -- handed to every waiter
                 entry.error = exc
                 with self._lock:
@@ -135,7 +135,8 @@ class CommitteeCache:
             raise entry.error
         stream = torch.cuda.current_stream()
         stream.wait_event(entry.ready)
-        for t in (entry.pre.kernel_lines, entry.pre.opening_keys, entry.pre.transformed_kernel):
+        for t in (entry.pre.kernel_lines, entry.pre.opening_keys, entry.pre.opening_lines,
+                  entry.pre.transformed_kernel):
             t.record_stream(stream)
         return entry.pre
 
@@ -222,7 +223,7 @@ def decrypt_group(dk: wb.PublicDecryptionKey, batches: Sequence, party_keys: Seq
     second = torch.cat([c.second[: GTB * B] if isinstance(c, wb.CiphertextBatch)
                         else wb.to_device(b"".join(x.second for x in c)) for c in batches])
     out = wb.empty_device(GTB * B * K)
-    ctx.call("wbte_wbtx_open_many", out, pre.opening_keys, sigmas, Ta, second, beta, valid, B, K)
+    ctx.call("wbte_wbtx_open_many", out, pre.opening_keys, pre.opening_lines, sigmas, Ta, second, beta, valid, B, K)
     if device_output:
         return [out[GTB * B * b : GTB * B * (b + 1)] for b in range(K)]
     host = wb.to_host(out, GTB * B * K)

@@ -658,6 +658,7 @@ class DecryptionPrecomputation:
     kernel_lines: object  # device, m * 68 * 288 bytes
     opening_keys: object  # device, B * T G2
     transformed_kernel: object  # device, m G2
+    opening_lines: object = None  # device, line tables of the B * T opening keys
 
     def batch_size(self) -> int:
         return self._batch_size
@@ -881,8 +882,11 @@ def prepare_decryption(decryption_key: PublicDecryptionKey,
             raise E.InvalidInterpolationSet() from exc
         raise
     ctx_id = decryption_context_id(decryption_key.setup_id(), B, parties)
+    # line tables of the opening keys, for the batched opening's multi-Miller loops
+    opening_lines = empty_device(_lib.LINE_BYTES * _lib.MILLER_LINES * B * len(parties))
+    _ctx().call("wbte_g2_prepare_lines", opening_lines, opening, B * len(parties))
     return DecryptionPrecomputation(decryption_key.setup_id(), ctx_id, B, accepted.accepted_weight(), parties, m,
-                                    lines, opening, kernel)
+                                    lines, opening, kernel, opening_lines)
 
 
 def _ensure_precomputation_batch(pre: DecryptionPrecomputation, batch: ValidatedBatch):
