@@ -46,6 +46,7 @@ extern "C" {
 #define WBTE_ERR_CUDA (-5)
 #define WBTE_ERR_NOT_ON_CURVE (-6)
 #define WBTE_ERR_INTERPOLATION (-7)
+#define WBTE_ERR_INTERNAL (-8)
 
 #define WBTE_FE_FULL 0
 #define WBTE_FE_EASY 1
@@ -189,6 +190,27 @@ int32_t wbte_lagrange_at_zero(wbte_ctx *ctx, void *out, const void *points, uint
  * weighted_btx/src/proof.rs:56-70); c_i is the Fiat-Shamir challenge. */
 int32_t wbte_schnorr_verify(wbte_ctx *ctx, uint8_t *valid, const void *X, const void *R,
                             const void *s, const void *c, uint64_t n);
+
+/* One field of a Fiat-Shamir transcript.  Record i contributes the len bytes
+ * at data + i * stride (stride 0: the same bytes for every record; data may
+ * be host or device memory).  kind 0: plain bytes; kind 1: a 289-byte
+ * wbte_gt_compress record, which contributes only its tag byte when the tag
+ * is 0 (append_gt of the identity, weighted_btx/src/encoding.rs:11-19). */
+typedef struct {
+    const void *data;
+    uint64_t stride;
+    uint32_t len;
+    uint32_t kind;
+} wbte_transcript_field;
+/* out[i] (32-byte canonical Fr) = the challenge of record i: the first
+ * SHA-256(field_0 || ... || field_{count-1} || counter u32 LE), counter =
+ * 0, 1, ..., whose little-endian value is below r -- challenge_scalar of
+ * btx/src/proof.rs:49-77, pfe/src/proof.rs:148-176,
+ * weighted_btx/src/proof.rs:72-100 and weighted_pfe/src/proof.rs:124-152
+ * (Sha256 + Scalar::from_bytes_le).  count <= 8.  WBTE_ERR_INTERNAL if a
+ * record exhausts 256 counters. */
+int32_t wbte_transcript_challenges(wbte_ctx *ctx, void *out, const wbte_transcript_field *fields, uint32_t count,
+                                   uint64_t n);
 
 /* ---------------------------------------------------- weighted_btx */
 typedef struct {

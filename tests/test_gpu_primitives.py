@@ -179,3 +179,52 @@ def test_schnorr_verify(orc):
     s[2] = (s[2] + 1) % orc.R
     ok = ops.schnorr_verify(b"".join(X), b"".join(Rc), s, c)
     assert list(ok) == [True, True, False, True, True, True]
+
+
+def _host_challenge(parts, R):
+    """Checker: SHA-256 rejection sampling over the concatenated parts."""
+    import hashlib
+    import struct
+
+    msg = b"".join(parts)
+    counter = 0
+    while True:
+        v = int.from_bytes(hashlib.sha256(msg + struct.pack("<I", counter)).digest(), "little")
+        if v < R:
+            return v
+        counter += 1
+
+
+@pytest.mark.parametrize("n", [1, 7, 300])
+def test_transcript_challenges_match_sha256(orc, n):
+    """Constant, fixed-stride and variable GT fields, record lengths crossing
+    the 64-byte block and padding boundaries, identity GT records."""
+    from weighted_bte_b200 import _lib
+
+    rng = random.Random(100 + n)
+    prefix = bytes(rng.randrange(256) for _ in range(rng.randrange(0, 130)))
+    a_len = rng.randrange(1, 70)
+    a = bytes(rng.randrange(256) for _ in range(a_len * n))
+    te = bytearray(rng.randrange(256) for _ in range(289 * n))
+    for i in range(n):
+        te[289 * i] = 0 if i % 3 == 1 else 1  # every third record is the identity
+    tail = bytes(rng.randrange(256) for _ in range(5))
+    fields = [(prefix, 0, len(prefix), _lib.TRANSCRIPT_BYTES), (a, a_len, a_len, _lib.TRANSCRIPT_BYTES),
+              (bytes(te), 289, 289, _lib.TRANSCRIPT_GT_VARIABLE), (tail, 0, 5, _lib.TRANSCRIPT_BYTES)]
+    got = ops.transcript_challenges(fields, n)
+    for i in range(n):
+        rec = bytes(te[289 * i : 289 * (i + 1)])
+        gt = rec[:1] if rec[0] == 0 else rec
+        assert got[i] == _host_challenge([prefix, a[a_len * i : a_len * (i + 1)], gt, tail], orc.R), i
+
+
+def test_transcript_challenges_exact_block_lengths(orc):
+    """Messages whose length before the counter is 55, 56, 60 and 64 bytes:
+    the padding edge cases of SHA-256."""
+    from weighted_bte_b200 import _lib
+
+    for total in (51, 52, 56, 60, 119, 120):
+        data = bytes((7 * i + total) & 0xFF for i in range(total * 3))
+        got = ops.transcript_challenges([(data, total, total, _lib.TRANSCRIPT_BYTES)], 3)
+        for i in range(3):
+            assert got[i] == _host_challenge([data[total * i : total * (i + 1)]], orc.R)

@@ -28,6 +28,7 @@ STATUS_NAMES = {
     -5: "WBTE_ERR_CUDA",
     -6: "WBTE_ERR_NOT_ON_CURVE",
     -7: "WBTE_ERR_INTERPOLATION",
+    -8: "WBTE_ERR_INTERNAL",
 }
 FE_FULL, FE_EASY, FE_HARD = 0, 1, 2
 CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
@@ -55,6 +56,20 @@ class WbtxKey(ctypes.Structure):
         ("total_weight", ctypes.c_uint64),
         ("max_batch_size", ctypes.c_uint64),
     ]
+
+
+class TranscriptField(ctypes.Structure):
+    """wbte_transcript_field: record i contributes `len` bytes at data + i * stride."""
+
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("stride", ctypes.c_uint64),
+        ("len", ctypes.c_uint32),
+        ("kind", ctypes.c_uint32),
+    ]
+
+
+TRANSCRIPT_BYTES, TRANSCRIPT_GT_VARIABLE = 0, 1
 
 
 class WpfeKey(ctypes.Structure):
@@ -100,6 +115,7 @@ _SIGNATURES = {
     "wbte_gt_compress": [_VP, _VP, _U64],
     "wbte_lagrange_at_zero": [_VP, _VP, _U64],
     "wbte_schnorr_verify": [_VP, _VP, _VP, _VP, _VP, _U64],
+    "wbte_transcript_challenges": [_VP, _VP, ctypes.c_uint32, _U64],
     "wbte_wbtx_partial_decrypt": [_VP, _VP, _U64, _VP, _U64],
     "wbte_wbtx_verify_shares": [_VP, _VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64],
     "wbte_wbtx_prepare": [_VP, _VP, _U64, _U64, _VP, _VP, _VP],

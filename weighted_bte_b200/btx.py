@@ -248,20 +248,18 @@ class Ciphertext:
 
 
 def _challenges(first_c: List[bytes], second_enc: List[bytes], comm_c: List[bytes]) -> List[int]:
-    """Fiat-Shamir challenge with rejection sampling (btx/src/proof.rs:52-77)."""
-    gen_c = ops.g1_compress(wb.g1_generator(), 1)
-    out = []
-    for a, b, c in zip(first_c, second_enc, comm_c):
-        prefix = TRANSCRIPT_DOMAIN + gen_c + a + b + c
-        counter = 0
-        while True:
-            d = hashlib.sha256(prefix + struct.pack("<I", counter)).digest()
-            v = int.from_bytes(d, "little")
-            if v < R:
-                out.append(v)
-                break
-            counter += 1
-    return out
+    """Fiat-Shamir challenges with rejection sampling (btx/src/proof.rs:49-77), hashed on
+    the device: domain, compressed generator, then per ciphertext its compressed
+    first component, GT encoding and compressed commitment."""
+    n = len(first_c)
+    if n == 0:
+        return []
+    prefix = TRANSCRIPT_DOMAIN + ops.g1_compress(wb.g1_generator(), 1)
+    te = b"".join(x if len(x) == 289 else x + bytes(289 - len(x)) for x in second_enc)
+    return ops.transcript_challenges([(prefix, 0, len(prefix), _lib.TRANSCRIPT_BYTES),
+                                      (b"".join(first_c), 48, 48, _lib.TRANSCRIPT_BYTES),
+                                      (te, 289, 289, _lib.TRANSCRIPT_GT_VARIABLE),
+                                      (b"".join(comm_c), 48, 48, _lib.TRANSCRIPT_BYTES)], n)
 
 
 def encrypt_many(encryption_key: EncryptionKey, messages: Sequence[bytes], rng) -> List[Ciphertext]:

@@ -137,6 +137,29 @@ void launch_unmask(uint8_t* out, const uint8_t* second, const uint8_t* alpha, co
 void launch_gt_compress(uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
 // flags[i] = (in[i] == 1)
 void launch_fp12_is_one(uint8_t* flags, const uint8_t* in, int64_t n, cudaStream_t s);
+// ------------------------------------------------------------ transcripts
+// One field of a Fiat-Shamir transcript: record i contributes the len bytes
+// at data + i * stride (stride 0: the same bytes for every record).  A
+// TRANSCRIPT_GT_VARIABLE field is a 289-byte compressed GT record that
+// contributes only its tag byte when the tag is 0 (the identity).
+enum TranscriptKind : uint32_t { TRANSCRIPT_BYTES = 0, TRANSCRIPT_GT_VARIABLE = 1 };
+constexpr int TRANSCRIPT_MAX_FIELDS = 8;
+constexpr uint32_t TRANSCRIPT_MAX_TRIES = 256;
+struct TranscriptField {
+    const uint8_t* data;
+    uint64_t stride;
+    uint32_t len;
+    uint32_t kind;
+};
+struct TranscriptSpec {
+    TranscriptField f[TRANSCRIPT_MAX_FIELDS];
+    int32_t count;
+};
+// out[i] (32-byte canonical scalar) = SHA-256 rejection-sampled challenge of
+// record i's fields followed by a u32 LE counter; *status = 1 if a record
+// ran out of counters
+void launch_transcript_challenges(uint8_t* out, const TranscriptSpec& spec, int64_t n, int32_t* status,
+                                  cudaStream_t s);
 // sustained 32-bit IMAD instructions per second (calibration kernel, synchronising)
 double measure_imad_rate(cudaStream_t s);
 

@@ -661,6 +661,37 @@ int32_t wbte_lagrange_at_zero(wbte_ctx* ctx, void* out, const void* points, uint
     if (c.to_host(&st, status, sizeof(st)) && st) c.fail(WBTE_ERR_INTERPOLATION, "the interpolation points must be nonempty and distinct");
     return c.finish();
 }
+int32_t wbte_transcript_challenges(wbte_ctx* ctx, void* out, const wbte_transcript_field* fields, uint32_t count,
+                                   uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !fields) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    if (count > (uint32_t)TRANSCRIPT_MAX_FIELDS) return c.fail(WBTE_ERR_SIZE, "at most 8 transcript fields");
+    TranscriptSpec spec{};
+    spec.count = (int32_t)count;
+    for (uint32_t k = 0; k < count; k++) {
+        const wbte_transcript_field& f = fields[k];
+        if (f.kind > TRANSCRIPT_GT_VARIABLE || (f.kind == TRANSCRIPT_GT_VARIABLE && f.len != 289))
+            return c.fail(WBTE_ERR_INVALID_ARG, "invalid transcript field kind");
+        if (f.len > (1u << 20)) return c.fail(WBTE_ERR_SIZE, "transcript field longer than 1 MiB");
+        if (f.len == 0) {
+            spec.f[k] = TranscriptField{nullptr, 0, 0, TRANSCRIPT_BYTES};
+            continue;
+        }
+        if (!f.data) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+        if (f.stride != 0 && f.stride < f.len) return c.fail(WBTE_ERR_INVALID_ARG, "transcript records overlap");
+        const size_t extent = f.stride == 0 ? f.len : f.stride * (n - 1) + f.len;
+        spec.f[k] = TranscriptField{c.in(f.data, extent), f.stride, f.len, f.kind};
+    }
+    uint8_t* d = c.out(out, FR_SZ * n);
+    int32_t* status = (int32_t*)c.zeros(sizeof(int32_t));
+    if (!c.ok()) return c.finish();
+    launch_transcript_challenges(d, spec, (int64_t)n, status, c.s);
+    int32_t st = 0;
+    if (c.to_host(&st, status, sizeof(st)) && st) c.fail(WBTE_ERR_INTERNAL, "challenge rejection sampling ran out of counters");
+    return c.finish();
+}
 int32_t wbte_schnorr_verify(wbte_ctx* ctx, uint8_t* valid, const void* X, const void* R, const void* s, const void* ch, uint64_t n) {
     if (!ctx) return WBTE_ERR_INVALID_ARG;
     Call c(ctx);

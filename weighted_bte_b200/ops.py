@@ -231,5 +231,26 @@ def schnorr_verify(X, Rc, s, c) -> np.ndarray:
     return out.astype(bool)
 
 
+def transcript_challenges(fields, n: int, out=None):
+    """Fiat-Shamir challenges of n records on the device (wbte_transcript_challenges).
+
+    `fields` lists (data, stride, length, kind) in transcript order: record i
+    contributes `length` bytes at data + i * stride (stride 0: constant bytes);
+    kind TRANSCRIPT_GT_VARIABLE marks 289-byte compressed GT records encoded
+    as one byte when they hold the identity.  Returns the scalars as ints, or
+    writes 32-byte canonical scalars into `out` (host or device) and returns it.
+    """
+    keep = _lib._Keep()
+    arr = (_lib.TranscriptField * max(1, len(fields)))()
+    for k, (data, stride, length, kind) in enumerate(fields):
+        arr[k].data = keep.ptr(data) if length else None
+        arr[k].stride, arr[k].len, arr[k].kind = int(stride), int(length), int(kind)
+    buf = out if out is not None else bytearray(32 * n)
+    ctx().call("wbte_transcript_challenges", buf, arr, len(fields), n)
+    if out is not None:
+        return out
+    return [int.from_bytes(buf[32 * i : 32 * i + 32], "little") for i in range(n)]
+
+
 def split(blob: bytes, size: int) -> list:
     return [bytes(blob[i : i + size]) for i in range(0, len(blob), size)]

@@ -200,19 +200,16 @@ class Ciphertext:
 
 
 def _challenges(rb_c: bytes, first_c, second_c, c1_c, c2_c) -> List[int]:
-    """Fiat-Shamir challenge with rejection sampling (pfe/src/proof.rs:148-176)."""
-    out = []
-    for a, b, c, d in zip(first_c, second_c, c1_c, c2_c):
-        prefix = TRANSCRIPT_DOMAIN + rb_c + a + b + c + d
-        counter = 0
-        while True:
-            h = hashlib.sha256(prefix + struct.pack("<I", counter)).digest()
-            v = int.from_bytes(h, "little")
-            if v < R:
-                out.append(v)
-                break
-            counter += 1
-    return out
+    """Fiat-Shamir challenges with rejection sampling (pfe/src/proof.rs:148-176), hashed on
+    the device: domain and compressed relation base, then per ciphertext four
+    compressed G1 points."""
+    n = len(first_c)
+    if n == 0:
+        return []
+    prefix = TRANSCRIPT_DOMAIN + rb_c
+    fields = [(prefix, 0, len(prefix), _lib.TRANSCRIPT_BYTES)]
+    fields += [(b"".join(x), 48, 48, _lib.TRANSCRIPT_BYTES) for x in (first_c, second_c, c1_c, c2_c)]
+    return ops.transcript_challenges(fields, n)
 
 
 def encrypt_many(encryption_key: EncryptionKey, messages: Sequence[bytes], rng) -> List[Ciphertext]:

@@ -427,21 +427,27 @@ class Ciphertext:
         return bool(verify_ciphertexts([self], encryption_key.setup_id())[0])
 
 
+def _transcript_prefix(setup_id: bytes) -> bytes:
+    return TRANSCRIPT_DOMAIN + setup_id + ops.g1_compress(g1_generator(), 1)
+
+
+def _challenge_fields(setup_id: bytes, first_c, second_enc, comm_c):
+    """Transcript fields of challenge_scalar (weighted_btx/src/proof.rs:72-100):
+    domain, setup id, compressed generator, then per ciphertext its compressed
+    first component, GT encoding and compressed commitment."""
+    prefix = _transcript_prefix(setup_id)
+    return [(prefix, 0, len(prefix), _lib.TRANSCRIPT_BYTES), (first_c, 48, 48, _lib.TRANSCRIPT_BYTES),
+            (second_enc, 289, 289, _lib.TRANSCRIPT_GT_VARIABLE), (comm_c, 48, 48, _lib.TRANSCRIPT_BYTES)]
+
+
 def _challenges(setup_id: bytes, first_c: List[bytes], second_enc: List[bytes], comm_c: List[bytes]) -> List[int]:
-    """Fiat-Shamir challenge with rejection sampling (weighted_btx/src/proof.rs:156-185)."""
-    gen_c = ops.g1_compress(g1_generator(), 1)
-    out = []
-    for a, b, c in zip(first_c, second_enc, comm_c):
-        prefix = TRANSCRIPT_DOMAIN + setup_id + gen_c + a + b + c
-        counter = 0
-        while True:
-            d = hashlib.sha256(prefix + struct.pack("<I", counter)).digest()
-            v = int.from_bytes(d, "little")
-            if v < R:
-                out.append(v)
-                break
-            counter += 1
-    return out
+    """Fiat-Shamir challenges with rejection sampling (weighted_btx/src/proof.rs:72-100),
+    hashed on the device; identity GT encodings (one byte) travel as 289-byte records."""
+    n = len(first_c)
+    if n == 0:
+        return []
+    te = b"".join(b if len(b) == 289 else b + bytes(289 - len(b)) for b in second_enc)
+    return ops.transcript_challenges(_challenge_fields(setup_id, b"".join(first_c), te, b"".join(comm_c)), n)
 
 
 def encrypt_many(encryption_key: EncryptionKey, messages: Sequence[bytes], rng) -> List[Ciphertext]:
@@ -492,6 +498,8 @@ class CiphertextBatch:
         self.responses = [int(r) for r in responses]
         self._enc = None
         self._digest = None
+        self._records = None
+        self._resp_bytes = None
 
     @classmethod
     def upload(cls, cts: Sequence[Ciphertext]) -> "CiphertextBatch":
@@ -507,24 +515,77 @@ class CiphertextBatch:
         return [Ciphertext(f[G1B * i : G1B * (i + 1)], s[GTB * i : GTB * (i + 1)],
                            SchnorrProof(c[G1B * i : G1B * (i + 1)], self.responses[i])) for i in range(n)]
 
+    def responses_bytes(self) -> bytes:
+        if self._resp_bytes is None:
+            self._resp_bytes = ops.scalars_bytes(self.responses)
+        return self._resp_bytes
+
+    def records(self) -> np.ndarray:
+        """Canonical per-ciphertext records (n x 417 bytes: compressed first,
+        GT encoding as a 289-byte record, compressed commitment, response),
+        encoded on the device."""
+        if self._records is None:
+            n = len(self)
+            fc, te, cc = _encode_on_device(self.first, self.commitment, self.second, n)
+            self._records = _records_host(fc, te, cc, to_device(self.responses_bytes()), n)
+        return self._records
+
     def encodings(self):
         if self._enc is None:
-            n = len(self)
-            first_c = ops.split(ops.g1_compress(self.first, n), 48)
-            comm_c = ops.split(ops.g1_compress(self.commitment, n), 48)
-            self._enc = (self.first, self.commitment, first_c, comm_c, append_gt_many(self.second, n))
+            self._enc = (self.first, self.commitment) + _encodings_of_records(self.records())
         return self._enc
 
     def digest(self) -> bytes:
         if self._digest is None:
-            _, _, first_c, comm_c, second_enc = self.encodings()
-            h = hashlib.sha256()
-            h.update(BATCH_DIGEST_DOMAIN)
-            h.update(struct.pack("<Q", len(self)))
-            for i, r in enumerate(self.responses):
-                h.update(_canonical(first_c[i], second_enc[i], comm_c[i], r))
-            self._digest = h.digest()
+            self._digest = _digest_of_records(self.records())
         return self._digest
+
+
+# one ciphertext's canonical record: compressed first component, GT record,
+# compressed commitment, response (weighted_btx/src/decryption.rs:740-748)
+RECORD_BYTES = 48 + 289 + 48 + 32
+_GT_AT, _COMM_AT, _RESP_AT = 48, 48 + 289, 48 + 289 + 48
+
+
+def _encode_on_device(first_dev, comm_dev, second_dev, n: int):
+    """Compressed first components, GT records and compressed commitments of
+    n ciphertexts, as device buffers."""
+    fc, cc, te = empty_device(48 * n), empty_device(48 * n), empty_device(289 * n)
+    ctx = _ctx()
+    ctx.call("wbte_g1_compress", fc, first_dev, n)
+    ctx.call("wbte_g1_compress", cc, comm_dev, n)
+    ctx.call("wbte_gt_compress", te, second_dev, n)
+    return fc, te, cc
+
+
+def _records_host(fc, te, cc, resp_dev, n: int) -> np.ndarray:
+    torch = _t()
+    rec = torch.cat([fc[: 48 * n].view(n, 48), te[: 289 * n].view(n, 289), cc[: 48 * n].view(n, 48),
+                     resp_dev[: 32 * n].view(n, 32)], 1)
+    return rec.cpu().numpy()
+
+
+def _encodings_of_records(rec: np.ndarray):
+    first_c = [bytes(r[:_GT_AT]) for r in rec]
+    comm_c = [bytes(r[_COMM_AT:_RESP_AT]) for r in rec]
+    second_enc = [bytes(r[_GT_AT:_COMM_AT]) if r[_GT_AT] else b"\x00" for r in rec]
+    return first_c, comm_c, second_enc
+
+
+def _digest_of_records(rec: np.ndarray) -> bytes:
+    """batch_digest over canonical records (weighted_btx/src/decryption.rs:740-748):
+    an identity GT contributes its tag byte only."""
+    h = hashlib.sha256()
+    h.update(BATCH_DIGEST_DOMAIN)
+    h.update(struct.pack("<Q", len(rec)))
+    ident = rec[:, _GT_AT] == 0
+    if ident.any():
+        keep = np.ones(rec.shape, dtype=bool)
+        keep[ident, _GT_AT + 1 : _COMM_AT] = False
+        h.update(rec[keep].tobytes())
+    else:
+        h.update(np.ascontiguousarray(rec).data)
+    return h.digest()
 
 
 def _encodings(cts):
@@ -690,25 +751,15 @@ def _validate_batch_size(dk: PublicDecryptionKey, batch_size: int):
 
 def validate_batch(decryption_key: PublicDecryptionKey, ciphertexts: Sequence[Ciphertext]) -> ValidatedBatch:
     """weighted_btx/src/decryption.rs:85-140: verify every proof, keep slot positions."""
-    _validate_batch_size(decryption_key, len(ciphertexts))
-    enc = _encodings(ciphertexts)
-    valid = verify_ciphertexts(ciphertexts, decryption_key.setup_id(), enc)
-    valid_dev = to_device(valid.astype(np.uint8).tobytes())
-    if isinstance(ciphertexts, CiphertextBatch):
-        n = len(ciphertexts)
-        first_dev = (ciphertexts.first[: G1B * n].view(n, G1B) * valid_dev[:n].view(n, 1)).reshape(-1)
-        first = None
-    else:
-        first = b"".join(ct.first if v else G1_IDENTITY for ct, v in zip(ciphertexts, valid))
-        first_dev = to_device(first)
-    return ValidatedBatch(decryption_key.setup_id(), len(ciphertexts), batch_digest(ciphertexts, enc),
-                          valid, first, first_dev, valid_dev)
+    return validate_batches(decryption_key, [ciphertexts])[0]
 
 
 def validate_batches(decryption_key: PublicDecryptionKey, batches: Sequence) -> List[ValidatedBatch]:
-    """`validate_batch` for several batches with one compression pass and one
-    proof-check launch over all their ciphertexts; each result equals
-    `validate_batch` of that batch alone."""
+    """`validate_batch` for several batches in one pass on the device: the
+    ciphertexts are encoded (compressed G1, GT records), hashed into their
+    Fiat-Shamir challenges and proof-checked with one launch each; each result
+    equals `validate_batch` of that batch alone.  The host only hashes the
+    canonical records into each batch digest."""
     if not batches:
         return []
     for cts in batches:
@@ -726,26 +777,31 @@ def validate_batches(decryption_key: PublicDecryptionKey, batches: Sequence) -> 
             return to_device(b"".join(c.proof.commitment for c in cts))
         return to_device(b"".join(c.second for c in cts))
 
+    def resp(cts):
+        return cts.responses_bytes() if isinstance(cts, CiphertextBatch) else ops.scalars_bytes(_responses(cts))
+
     first_all = torch.cat([dev(cts, "first", G1B) for cts in batches])
     comm_all = torch.cat([dev(cts, "commitment", G1B) for cts in batches])
     second_all = torch.cat([dev(cts, "second", GTB) for cts in batches])
-    first_c = ops.split(ops.g1_compress(first_all, total), 48)
-    comm_c = ops.split(ops.g1_compress(comm_all, total), 48)
-    second_enc = append_gt_many(second_all, total)
-    responses = [r for cts in batches for r in _responses(cts)]
-    cs = _challenges(decryption_key.setup_id(), first_c, second_enc, comm_c)
+    resp_all = to_device(b"".join(resp(cts) for cts in batches))
+    fc, te, cc = _encode_on_device(first_all, comm_all, second_all, total)
+    ch = empty_device(32 * total)
+    ops.transcript_challenges(_challenge_fields(decryption_key.setup_id(), fc, te, cc), total, out=ch)
     ok = np.zeros(total, dtype=np.uint8)
-    ops.ctx().call("wbte_schnorr_verify", ok, first_all, comm_all, ops.scalars_bytes(responses), ops.scalars_bytes(cs),
-                   total)
+    _ctx().call("wbte_schnorr_verify", ok, first_all, comm_all, resp_all, ch, total)
+    records = _records_host(fc, te, cc, resp_all, total)
     valid_all = ok.astype(bool)
     valid_dev_all = to_device(ok.tobytes())
     first_masked = (first_all.view(total, G1B) * valid_dev_all[:total].view(total, 1)).reshape(-1)
     out, o = [], 0
     for cts, n in zip(batches, sizes):
-        enc = (None, None, first_c[o : o + n], comm_c[o : o + n], second_enc[o : o + n])
-        if isinstance(cts, CiphertextBatch) and cts._digest is None:
-            cts._enc = (cts.first, cts.commitment) + enc[2:]
-        digest = batch_digest(cts, enc)
+        rec = records[o : o + n]
+        if isinstance(cts, CiphertextBatch):
+            if cts._records is None:
+                cts._records = rec
+            digest = cts.digest()
+        else:
+            digest = _digest_of_records(rec)
         out.append(ValidatedBatch(decryption_key.setup_id(), n, digest, valid_all[o : o + n], None,
                                   first_masked[G1B * o : G1B * (o + n)], valid_dev_all[o : o + n]))
         o += n

@@ -335,20 +335,20 @@ def _encodings(cts):
 
 
 def _challenges(setup_id: bytes, first_c, comm_c, targets) -> List[int]:
-    """Fiat-Shamir challenge with rejection sampling (weighted_pfe/src/proof.rs:124-152)."""
-    gen_c = ops.g1_compress(wb.g1_generator(), 1)
-    out = []
-    for a, c, tgt in zip(first_c, comm_c, targets):
-        prefix = TRANSCRIPT_DOMAIN + setup_id + gen_c + a + struct.pack("<Q", len(tgt)) + tgt + c
-        counter = 0
-        while True:
-            d = hashlib.sha256(prefix + struct.pack("<I", counter)).digest()
-            v = int.from_bytes(d, "little")
-            if v < R:
-                out.append(v)
-                break
-            counter += 1
-    return out
+    """Fiat-Shamir challenges with rejection sampling (weighted_pfe/src/proof.rs:124-152),
+    hashed on the device: domain, setup id, compressed generator, then per
+    ciphertext its compressed first component, the encoded target's length
+    (u64 LE, always 289) and fixed-width encoding, and the compressed commitment."""
+    n = len(first_c)
+    if n == 0:
+        return []
+    prefix = TRANSCRIPT_DOMAIN + setup_id + ops.g1_compress(wb.g1_generator(), 1)
+    tlen = struct.pack("<Q", 289)
+    return ops.transcript_challenges([(prefix, 0, len(prefix), _lib.TRANSCRIPT_BYTES),
+                                      (b"".join(first_c), 48, 48, _lib.TRANSCRIPT_BYTES),
+                                      (tlen, 0, 8, _lib.TRANSCRIPT_BYTES),
+                                      (b"".join(targets), 289, 289, _lib.TRANSCRIPT_BYTES),
+                                      (b"".join(comm_c), 48, 48, _lib.TRANSCRIPT_BYTES)], n)
 
 
 def encrypt_many(encryption_key: EncryptionKey, messages: Sequence[bytes], rng) -> List[Ciphertext]:
