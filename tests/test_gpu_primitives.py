@@ -144,8 +144,13 @@ def test_group_ntt_matches_oracle(orc, n):
         assert ops.split(ops.g2_ntt(b"".join(g2), inverse=inv), 192) == orc.g2_ntt(g2, inverse=inv)
 
 
+@pytest.mark.parametrize("lanes", ["auto", "1", "2"])
 @pytest.mark.parametrize("n", [2, 4, 8, 16, 32])
-def test_gt_transforms_match_oracle(orc, n):
+def test_gt_transforms_match_oracle(orc, n, lanes, monkeypatch):
+    """Radix-2 and radix-4 stages; the radix-4 twiddle powers on one, two or
+    four lanes per exponentiation (auto picks four at these sizes)."""
+    if lanes != "auto":
+        monkeypatch.setenv("WBTE_GT_LANES", lanes)
     rng = random.Random(400 + n)
     e = orc.pairing(orc.g1_generator(), orc.g2_generator())
     vals = orc.gt_pow_many(e, rs(rng, n, orc.R))

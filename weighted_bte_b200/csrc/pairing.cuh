@@ -381,6 +381,44 @@ static __device__ __noinline__ void gt_pow_lane(Fp12& out, const Fp12& v, uint64
     out = acc;
 }
 
+// out = prod over the digits c = c0, c0 + step, ... < 4 of v^(d_c |x|^c):
+// one run of 64 cyclotomic squarings shared by the selected digits (Straus),
+// over one table of powers of phi^c0(v), phi = conj o Frobenius acting as
+// |x|; a later digit c applies phi^(c - c0) to the entry it multiplies in.
+// step 4 is gt_pow_lane (one digit); step 1 is the whole exponentiation.
+static __device__ __noinline__ void gt_pow_digits(Fp12& out, const Fp12& v, const uint64_t d[4], int c0, int step) {
+    Fp12 tab[8];  // phi^c0(v)^1 .. ^8
+    if (c0 == 0) {
+        tab[0] = v;
+    } else {
+        fp12_frobenius(tab[0], v, c0);
+        if (c0 & 1) fp12_conj(tab[0], tab[0]);
+    }
+    fp12_cyclotomic_sqr(tab[1], tab[0]);
+    for (int k = 2; k < 8; k++) fp12_mul(tab[k], tab[k - 1], tab[0]);
+    Fp12 acc = fp12_one();
+    for (int k = 16; k >= 0; k--) {
+        if (k != 16) {
+            fp12_cyclotomic_sqr(acc, acc);
+            fp12_cyclotomic_sqr(acc, acc);
+            fp12_cyclotomic_sqr(acc, acc);
+            fp12_cyclotomic_sqr(acc, acc);
+        }
+        for (int c = c0; c < 4; c += step) {
+            const int dd = r16_digit(d[c], 0, k, 16);
+            const int ad = dd < 0 ? -dd : dd;
+            if (!ad) continue;
+            const int rel = c - c0;
+            Fp12 m;
+            if (rel == 0) m = tab[ad - 1];
+            else fp12_frobenius(m, tab[ad - 1], rel);
+            if (((rel & 1) != 0) != (dd < 0)) fp12_conj(m, m);
+            fp12_mul(acc, acc, m);
+        }
+    }
+    out = acc;
+}
+
 // out = [w]p for w = hi 2^64 + lo < 16^top, over the signed radix-16 digits
 template <class F>
 static __device__ __noinline__ void xyzz_mul_r16(Xyzz<F>& out, const Xyzz<F>& p, uint64_t lo, uint64_t hi, int top) {
