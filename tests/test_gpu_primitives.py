@@ -76,6 +76,34 @@ def test_msm_family_indexed_and_vectors(orc, pts):
             assert got[j] == msm(pj, sj), (group, j)
 
 
+@pytest.mark.parametrize("lanes", ["auto", "1", "2", "4", "8", "16"])
+def test_small_msm_lanes_match_oracle(orc, pts, lanes, monkeypatch):
+    """The few-term MSM path (n <= 4) with every lane split: edge scalars
+    (0, 1, r - 1), identity points, an output count off the warp size."""
+    if lanes != "auto":
+        monkeypatch.setenv("WBTE_SMALL_MSM_LANES", lanes)
+    g1, g2 = pts
+    rng = random.Random(31)
+    for n in (1, 2, 3, 4):
+        k, V = 37, 3
+        idx = rng.sample(range(16), n)
+        base = [rng.randrange(0, 40) for _ in range(k)]
+        vsel = [rng.randrange(V) for _ in range(k)]
+        scal = rs(rng, V * n, orc.R)
+        scal[0], scal[-1] = 0, orc.R - 1
+        if n > 1:
+            scal[1] = 1
+        for group, bank, size, msm, ident in ((1, g1, 96, orc.g1_msm, orc.G1_IDENTITY),
+                                              (2, g2, 192, orc.g2_msm, bytes(192))):
+            bank = list(bank)
+            bank[base[2] + idx[0]] = ident
+            got = ops.split(ops.msm_family(group, b"".join(bank), len(bank), base, idx, scal, vsel, V, n), size)
+            for j in range(k):
+                pj = [bank[base[j] + t] for t in idx]
+                sj = scal[vsel[j] * n : (vsel[j] + 1) * n]
+                assert got[j] == msm(pj, sj), (group, n, j)
+
+
 def test_compressed_encodings_match_oracle(orc, pts):
     g1, g2 = pts
     g1 = g1[:8] + [orc.G1_IDENTITY]

@@ -1,5 +1,7 @@
 // Scalar-field kernels, batched point multiplication, radix-2 group
 // transforms, compressed encodings and Schnorr checks.
+#include <algorithm>
+#include <cstdlib>
 #include <mutex>
 
 #include "launch.h"
@@ -281,19 +283,65 @@ __global__ void __launch_bounds__(WARP) k_ntt_stage(uint8_t* work, const uint8_t
 }
 
 // MSMs of a few terms (the share checks' per-slot aggregates): out[o] =
-// sum_t scalars[vsel[o] n + t] points[pbase[o] + idx[t]], each term multiplied
-// directly with the lane split of the transforms (L lanes per output, one
-// base-|x| digit group each) and the parts summed across the lanes.  Every
-// output costs L threads; Pippenger's windows and window combine would cost
-// more than the terms themselves at this size.
+// sum_t scalars[vsel[o] n + t] points[pbase[o] + idx[t]].  Every scalar is
+// split into base-|x| digit groups (G2: four 64-bit digits, digit c acting
+// on (-1)^c psi^c(v); G1: two 128-bit digits acting on v and phi(v) + v), and
+// the (term, digit) pairs of one output are spread over L lanes.  Each lane
+// runs one signed radix-16 Straus loop over its pairs -- one run of
+// doublings shared by all of them -- and the lanes' sums meet in shared
+// memory.  L = 1 does the least work; more lanes cut the latency of small
+// launches.  Pippenger's windows would cost more than the terms here.
+template <class F> struct SmallMsmDigits;
+template <> struct SmallMsmDigits<Fp2> { static constexpr int D = 4, TOP = 16, TABS = 1; };
+template <> struct SmallMsmDigits<Fp> { static constexpr int D = 2, TOP = 32, TABS = 2; };
+
+WBTE_INL void small_msm_digits(uint64_t lo[4], uint64_t hi[4], const uint64_t d[4], const G2X*) {
+    for (int c = 0; c < 4; c++) {
+        lo[c] = d[c];
+        hi[c] = 0;
+    }
+}
+// G1: w_c = d_{2c} + d_{2c+1} |x| as 128-bit integers (s = w_0 + w_1 |x|^2)
+WBTE_INL void small_msm_digits(uint64_t lo[4], uint64_t hi[4], const uint64_t d[4], const G1X*) {
+    for (int c = 0; c < 2; c++) {
+        const uint64_t plo = d[2 * c + 1] * X_ABS, phi = __umul64hi(d[2 * c + 1], X_ABS);
+        lo[c] = plo + d[2 * c];
+        hi[c] = phi + (lo[c] < plo ? 1 : 0);
+    }
+}
+template <class F>
+WBTE_INL void small_msm_table(Xyzz<F>* tab, const Xyzz<F>& v) {  // tab[m] = [m + 1] v
+    tab[0] = v;
+    tab[1] = xyzz_dbl(v);
+    for (int m = 2; m < 8; m++) tab[m] = xyzz_add(tab[m - 1], v);
+}
+WBTE_INL void small_msm_tables(G2X tab[1][8], const G2X& v) { small_msm_table(tab[0], v); }
+WBTE_INL void small_msm_tables(G1X tab[2][8], const G1X& v) {
+    small_msm_table(tab[0], v);
+    small_msm_table(tab[1], xyzz_add(g1_phi(v), v));
+}
+// [dd] times the digit-c base, dd != 0
+WBTE_INL G2X small_msm_entry(const G2X tab[1][8], int c, int dd) {
+    G2X m = tab[0][(dd < 0 ? -dd : dd) - 1];
+    for (int i = 0; i < c; i++) m = g2_psi(m);
+    if (((c & 1) != 0) != (dd < 0)) m = neg(m);
+    return m;
+}
+WBTE_INL G1X small_msm_entry(const G1X tab[2][8], int c, int dd) {
+    G1X m = tab[c][(dd < 0 ? -dd : dd) - 1];
+    if (dd < 0) m = neg(m);
+    return m;
+}
+
 template <class F>
 __global__ void __launch_bounds__(WARP) k_small_msm(uint8_t* out, const uint8_t* points, const int64_t* pbase,
                                                    const int32_t* idx, const uint8_t* scalars, const int32_t* vsel,
-                                                   int64_t k, int64_t n) {
-    constexpr int L = NttLanes<F>::L;
+                                                   int64_t k, int64_t n, int L) {
+    using S = SmallMsmDigits<F>;
+    constexpr int D = S::D;
     using A = Affine<F>;
     __shared__ Xyzz<F> sh[WARP];
-    const int lane = threadIdx.x, c = lane % L;
+    const int lane = threadIdx.x, sub = lane % L;
     const int64_t o = ((int64_t)blockIdx.x * WARP + lane) / L;
     const bool active = o < k;
     Xyzz<F> acc;
@@ -301,24 +349,43 @@ __global__ void __launch_bounds__(WARP) k_small_msm(uint8_t* out, const uint8_t*
     if (active) {
         const int64_t v = vsel ? (int64_t)vsel[o] : 0;
         const A* P = reinterpret_cast<const A*>(points) + pbase[o];
-        for (int64_t t = 0; t < n; t++) {
-            Xyzz<F> base = from_affine(load_affine(P + (idx ? (int64_t)idx[t] : t)));
-            uint32_t s[8];
-            load_scalar(s, scalars + FR_SZ * (v * n + t));
+        Xyzz<F> tab[SMALL_MSM_MAX][S::TABS][8];
+        uint64_t lo[SMALL_MSM_MAX][4], hi[SMALL_MSM_MAX][4];
+        // this lane's pairs p = sub, sub + L, ... (term p / D, digit p % D):
+        // every lane of a warp runs the same iterations, so the warp stays converged
+        int prev = -1;
+        for (int p = sub; p < n * D; p += L) {
+            const int t = p / D;
+            if (t == prev) continue;
+            prev = t;
+            small_msm_tables(tab[t], from_affine(load_affine(P + (idx ? (int64_t)idx[t] : t))));
+            uint32_t sc[8];
+            load_scalar(sc, scalars + FR_SZ * (v * n + t));
             uint64_t d[4];
-            decompose_base_x(d, s);
-            Xyzz<F> part;
-            ntt_part(part, base, d, c);
-            acc = xyzz_add(acc, part);
+            decompose_base_x(d, sc);
+            small_msm_digits(lo[t], hi[t], d, (const Xyzz<F>*)nullptr);
+        }
+        for (int kk = S::TOP; kk >= 0; kk--) {
+            if (kk != S::TOP) {
+                acc = xyzz_dbl(acc);
+                acc = xyzz_dbl(acc);
+                acc = xyzz_dbl(acc);
+                acc = xyzz_dbl(acc);
+            }
+            for (int p = sub; p < n * D; p += L) {
+                const int t = p / D, c = p % D;
+                const int dd = r16_digit(lo[t][c], hi[t][c], kk, S::TOP);
+                if (dd) acc = xyzz_add(acc, small_msm_entry(tab[t], c, dd));
+            }
         }
     }
     store_vec(sh + lane, acc);
     __syncwarp();
     for (int step = 1; step < L; step *= 2) {
-        if (c % (2 * step) == 0) store_vec(sh + lane, xyzz_add(load_vec(sh + lane), load_vec(sh + lane + step)));
+        if (sub % (2 * step) == 0) store_vec(sh + lane, xyzz_add(load_vec(sh + lane), load_vec(sh + lane + step)));
         __syncwarp();
     }
-    if (active && c == 0)
+    if (active && sub == 0)
         store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * o), to_affine(load_vec(sh + lane)));
 }
 
@@ -573,15 +640,59 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
     }
 }
 
+// Lanes per small-MSM output, from a cost model: a lane's work is its
+// tables (7 additions per term it touches; 15 on G1, two tables), the shared
+// doublings and one addition per window and pair it holds; the launch takes
+// about max(1, k L / resident threads) times one lane's work.  The lanes run
+// from 1 up to one per (term, digit) pair, rounded up to a power of two.
+// WBTE_SMALL_MSM_LANES (a power of two up to 32) overrides the choice.
+static int small_msm_lanes(Group g, int64_t k, int64_t n) {
+    if (const char* env = getenv("WBTE_SMALL_MSM_LANES")) {
+        const int v = atoi(env);
+        if (v >= 1 && v <= WARP && (v & (v - 1)) == 0) return v;
+    }
+    static std::atomic<int64_t> cap[2] = {{0}, {0}};
+    const int gi = g == GROUP_G1 ? 0 : 1;
+    int64_t c = cap[gi].load();
+    if (c == 0) {
+        int dev = 0, sms = 0, blocks = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g == GROUP_G1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_small_msm<Fp>, WARP, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_small_msm<Fp2>, WARP, 0);
+        c = (int64_t)(blocks > 0 ? blocks : 1) * WARP * (sms > 0 ? sms : 1);
+        cap[gi].store(c);
+    }
+    const bool g1 = g == GROUP_G1;
+    const int D = g1 ? SmallMsmDigits<Fp>::D : SmallMsmDigits<Fp2>::D;
+    const int windows = (g1 ? SmallMsmDigits<Fp>::TOP : SmallMsmDigits<Fp2>::TOP) + 1;
+    const double add = g1 ? 12.0 : 42.0, dbl = g1 ? 9.0 : 30.0, table = g1 ? 15.0 : 7.0;  // Fp products
+    const int64_t pairs = n * D;
+    int best = 1;
+    double best_t = 0;
+    for (int L = 1; L <= WARP; L *= 2) {
+        int terms = 0, prev = -1;
+        for (int64_t p = 0; p < pairs; p += L)
+            if (p / D != prev) prev = (int)(p / D), terms++;
+        const double lane = terms * table * add + 4.0 * (windows - 1) * dbl + (double)((pairs + L - 1) / L) * windows * add;
+        const double t = std::max(1.0, (double)(k * L) / (double)c) * lane;
+        if (L == 1 || t < best_t) best = L, best_t = t;
+        if (L >= pairs) break;
+    }
+    return best;
+}
+
 void launch_small_msm(Group g, uint8_t* out, const uint8_t* points, const int64_t* pbase, const int32_t* idx,
                       const uint8_t* scalars, const int32_t* vsel, int64_t k, int64_t n, cudaStream_t s) {
     ProfScope prof_(g == GROUP_G1 ? "small_msm_g1" : "small_msm_g2", s);
     if (k <= 0) return;
+    if (n < 1 || n > SMALL_MSM_MAX) return;
+    const int L = small_msm_lanes(g, k, n);
     note_launch();
     if (g == GROUP_G1)
-        k_small_msm<Fp><<<blocks_for(NttLanes<Fp>::L * k, WARP), WARP, 0, s>>>(out, points, pbase, idx, scalars, vsel, k, n);
+        k_small_msm<Fp><<<blocks_for(L * k, WARP), WARP, 0, s>>>(out, points, pbase, idx, scalars, vsel, k, n, L);
     else
-        k_small_msm<Fp2><<<blocks_for(NttLanes<Fp2>::L * k, WARP), WARP, 0, s>>>(out, points, pbase, idx, scalars, vsel, k, n);
+        k_small_msm<Fp2><<<blocks_for(L * k, WARP), WARP, 0, s>>>(out, points, pbase, idx, scalars, vsel, k, n, L);
 }
 
 void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {

@@ -1,6 +1,7 @@
 // Pairing-side kernels: G2 line tables, Miller loops, split final
 // exponentiation, the cyclotomic/GT radix-2 transforms and GT
 // exponentiation.
+#include <algorithm>
 #include <cstdlib>
 
 #include "launch.h"
@@ -483,9 +484,11 @@ void launch_final_exp(uint8_t* out, const uint8_t* in, int64_t n, FinalExpMode m
     k_final_exp<<<blocks_for(n), TPB, 0, s>>>(out, in, n, (int)mode);
 }
 
-// Lanes per exponentiation for a radix-4 stage of E twiddle powers: one
-// (the least work) once E fills the GPU's resident threads, else two or four
-// for parallelism.  WBTE_GT_LANES = 1, 2 or 4 overrides the choice.
+// Lanes per exponentiation for a radix-4 stage of E twiddle powers, from a
+// cost model: one lane's work in Fp products (65 squarings and 74 products
+// for all four digits on one lane; 65 and 40 on each of two; 65 and 25 on
+// each of four, with the Frobenius maps and the lane combine) times
+// max(1, E L / resident threads).  WBTE_GT_LANES = 1, 2 or 4 overrides it.
 static int gt_pow_lanes(int64_t E) {
     static std::atomic<int64_t> cap{0};
     if (const char* env = getenv("WBTE_GT_LANES")) {
@@ -501,9 +504,14 @@ static int gt_pow_lanes(int64_t E) {
         c = (int64_t)(blocks > 0 ? blocks : 1) * WARP * (sms > 0 ? sms : 1);
         cap.store(c);
     }
-    if (E >= c) return 1;
-    if (2 * E >= c) return 2;
-    return 4;
+    const double work[3] = {5829.0, 3560.0, 2533.0};
+    int best = 1;
+    double best_t = 0;
+    for (int i = 0, L = 1; L <= GT_LANES; i++, L *= 2) {
+        const double t = std::max(1.0, (double)(E * L) / (double)c) * work[i];
+        if (L == 1 || t < best_t) best = L, best_t = t;
+    }
+    return best;
 }
 
 static void gt_transform(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count, bool prefix, cudaStream_t s,

@@ -84,8 +84,9 @@ struct MsmPlan {
     int64_t segment = 0, segments = 0;
 };
 MsmPlan msm_plan(Group g, int64_t n, int64_t k);
-// MSMs of at most SMALL_MSM_MAX terms, computed term by term with lane-split
-// scalar multiplication (launch_msm_family dispatches here).
+// MSMs of at most SMALL_MSM_MAX terms by a Straus loop over the base-|x|
+// digits of every term, the digit pairs spread over 1..16 lanes per output
+// (launch_msm_family dispatches here).
 constexpr int64_t SMALL_MSM_MAX = 4;
 void launch_small_msm(Group g, uint8_t* out, const uint8_t* points, const int64_t* pbase, const int32_t* idx,
                       const uint8_t* scalars, const int32_t* vsel, int64_t k, int64_t n, cudaStream_t s);
