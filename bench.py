@@ -58,6 +58,11 @@ FP_MULS_PER_G2_MADD = 8 * 3 + 2 * 2
 METRIC = "ciphertexts decrypted/s (weighted_btx batch decryption, B=512)"
 
 
+# DRAM bytes (read + write) of one k_gt_radix4_pows<1> launch at this workload
+# (second radix-4 stage, 64 transforms of m = 1024), from one ncu capture
+NCU_GT_POWS_DRAM_BYTES = 17.822836e9 + 10.396248e9
+
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -426,18 +431,25 @@ def main():
     top_g = max(prof_g.items(), key=lambda kv: kv[1][0])
     gt_ms = prof_g.get("gt_ifft", (0.0, 0))[0]
     m = wb.transform_size_for(B)
-    roofline = {"kernel": "gt_ifft (k_gt_radix4: truncated cyclotomic inverse transform, batched form)",
+    roofline = {"kernel": "gt_ifft (truncated cyclotomic inverse transform, batched form: k_gt_radix4_pows + "
+                          "k_gt_radix4_outputs per radix-4 stage)",
                 "bound": "int", "unit": "G Fp products/s",
                 "peak_basis": f"measured {float(rate[0]) / 1e12:.2f} T IMAD/s (calibration kernel, mad.lo/mad.hi "
                               f"mix) / {IMAD_PER_FP_MUL} IMAD per Fp product",
-                "traffic": None, "peak": peak_fp / 1e9}
+                "traffic": NCU_GT_POWS_DRAM_BYTES if G == 64 and B == 512 else None,
+                "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one k_gt_radix4_pows<1> launch "
+                                 "(radix-4 stage h=16 of 64 transforms, m=1024) from one ncu capture of this "
+                                 "workload; the per-thread stack (tables, spills), against 2 x 576 B of "
+                                 "algorithmic input and output per exponentiation",
+                "peak": peak_fp / 1e9}
     if gt_ms > 0 and m == work["cyclotomic_prefix_ifft"]["m"] and B == work["cyclotomic_prefix_ifft"]["outputs"]:
         algo = G * work["cyclotomic_prefix_ifft"]["fp_products"]
         achieved = algo / (gt_ms / 1000.0)
         roofline.update({"achieved": achieved / 1e9, "frac": achieved / peak_fp,
                          "algorithmic_fp_products_per_launch_sequence": algo, "batches_per_launch": G,
                          "ms": gt_ms, "work_source": "oracle count of the reference algorithm (radix-2, "
-                         "decomposed plans); the kernel does 25% fewer exponentiations (radix-4)",
+                         "decomposed wNAF plans); the kernels do 25% fewer exponentiations (radix-4) on a "
+                         "fixed radix-16 schedule shared by the four digits",
                          "dominant_in_group": top_g[0] == "gt_ifft"})
     else:
         roofline.update({"achieved": None, "frac": None})
