@@ -152,6 +152,12 @@ int32_t wbte_gt_ntt(wbte_ctx *ctx, void *io, uint64_t n, int32_t inverse);
  * the first out_count outputs are valid afterwards
  * (ifft_cyclotomic_prefix_unscaled, btx/src/fft.rs:284-350). */
 int32_t wbte_gt_cyclotomic_prefix_ifft(wbte_ctx *ctx, void *io, uint64_t n, uint64_t out_count);
+/* The two transforms above over count independent arrays of n values laid
+ * back to back (array q at io + q * n * 576 bytes), one launch per stage for
+ * all of them: the batched form of the reference's per-batch transforms. */
+int32_t wbte_gt_ntt_many(wbte_ctx *ctx, void *io, uint64_t n, uint64_t count, int32_t inverse);
+int32_t wbte_gt_cyclotomic_prefix_ifft_many(wbte_ctx *ctx, void *io, uint64_t n, uint64_t out_count,
+                                            uint64_t count);
 
 /* ----------------------------------------------------------- pairing */
 /* Line tables of n G2 points: 68 lines x 288 bytes each, laid out

@@ -194,6 +194,32 @@ def test_gt_transforms_match_oracle(orc, n, lanes, monkeypatch):
     assert got == expect
 
 
+@pytest.mark.parametrize("count,lanes", [(32, "auto"), (32, "1"), (32, "2"), (33, "1"), (32, "4")])
+def test_gt_transforms_many_match_oracle(orc, count, lanes, monkeypatch):
+    """Batches of transforms in one launch per stage: 32 arrays give every
+    warp one twiddle power (the warp-uniform NAF plan), 33 arrays mix
+    twiddles within warps (the fixed schedule)."""
+    if lanes != "auto":
+        monkeypatch.setenv("WBTE_GT_LANES", lanes)
+    rng = random.Random(700 + count)
+    e = orc.pairing(orc.g1_generator(), orc.g2_generator())
+    n = 16
+    vals = orc.gt_pow_many(e, rs(rng, n * count, orc.R))
+    for inv in (False, True):
+        got = ops.split(ops.gt_ntt_many(b"".join(vals), n, inverse=inv), 576)
+        for q in range(count):
+            assert got[n * q : n * (q + 1)] == orc.gt_ntt(vals[n * q : n * (q + 1)], inverse=inv), (inv, q)
+    # truncated cyclotomic transforms agree after the hard part
+    m = 8
+    g1 = orc.g1_mul_many(orc.g1_generator(), rs(rng, m * count, orc.R))
+    g2 = orc.g2_mul_many(orc.g2_generator(), rs(rng, m, orc.R))
+    easy = [orc.easy_final_exp(orc.miller_loop(a, g2[i % m])) for i, a in enumerate(g1)]
+    got = ops.cyclotomic_prefix_ifft_many(b"".join(easy), m, m // 2)
+    for q in range(count):
+        hard = ops.split(ops.final_exp(got[q], mode=2), 576)
+        assert hard == orc.hard_final_exp_many(orc.cyclotomic_prefix_ifft(easy[m * q : m * (q + 1)], m // 2)), q
+
+
 def test_lagrange_matches_oracle(orc):
     rng = random.Random(6)
     xs = rs(rng, 70, orc.R)

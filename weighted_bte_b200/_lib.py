@@ -104,6 +104,8 @@ _SIGNATURES = {
     "wbte_g1_ntt": [_VP, _U64, _I32],
     "wbte_g2_ntt": [_VP, _U64, _I32],
     "wbte_gt_ntt": [_VP, _U64, _I32],
+    "wbte_gt_ntt_many": [_VP, _U64, _U64, _I32],
+    "wbte_gt_cyclotomic_prefix_ifft_many": [_VP, _U64, _U64, _U64],
     "wbte_gt_cyclotomic_prefix_ifft": [_VP, _U64, _U64],
     "wbte_g2_prepare_lines": [_VP, _VP, _U64],
     "wbte_miller_loop_lines": [_VP, _VP, _VP, _U64],

@@ -549,6 +549,34 @@ int32_t wbte_gt_cyclotomic_prefix_ifft(wbte_ctx* ctx, void* io, uint64_t n, uint
     return c.finish();
 }
 
+int32_t wbte_gt_ntt_many(wbte_ctx* ctx, void* io, uint64_t n, uint64_t count, int32_t inverse) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (count == 0) return c.finish();
+    if (!io) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    int lg = log2_exact(n);
+    if (n == 0 || lg < 0 || lg > 32) return c.fail(WBTE_ERR_SIZE, "transform size must be a power of two <= 2^32");
+    if (n == 1) return c.finish();
+    uint8_t* d = c.inout(io, GT_SZ * n * count);
+    const uint8_t* tw = twiddles(c, (int64_t)n, inverse != 0);
+    if (c.ok()) launch_gt_ntt(d, tw, (int64_t)n, c.s, (int64_t)count, inverse != 0);
+    return c.finish();
+}
+
+int32_t wbte_gt_cyclotomic_prefix_ifft_many(wbte_ctx* ctx, void* io, uint64_t n, uint64_t out_count, uint64_t count) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (count == 0) return c.finish();
+    if (!io) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    int lg = log2_exact(n);
+    if (n < 2 || lg < 0 || lg > 32) return c.fail(WBTE_ERR_SIZE, "transform size must be a power of two in [2, 2^32]");
+    if (out_count > n / 2) return c.fail(WBTE_ERR_SIZE, "out_count must be at most n / 2");
+    uint8_t* d = c.inout(io, GT_SZ * n * count);
+    const uint8_t* tw = twiddles(c, (int64_t)n, true);
+    if (c.ok()) launch_cyclotomic_prefix_ifft(d, tw, (int64_t)n, (int64_t)out_count, c.s, (int64_t)count);
+    return c.finish();
+}
+
 // -------------------------------------------------------------- pairing
 int32_t wbte_g2_prepare_lines(wbte_ctx* ctx, void* lines, const void* q, uint64_t n) {
     if (!ctx) return WBTE_ERR_INVALID_ARG;

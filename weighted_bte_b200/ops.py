@@ -147,6 +147,22 @@ def gt_ntt(values, inverse=False):
     return bytes(buf)
 
 
+def gt_ntt_many(values, n: int, inverse=False):
+    """`gt_ntt` of len(values) / (576 n) arrays of n values laid back to back."""
+    buf = bytearray(values)
+    ctx().call("wbte_gt_ntt_many", buf, n, len(buf) // (GT_BYTES * n), int(inverse))
+    return bytes(buf)
+
+
+def cyclotomic_prefix_ifft_many(values, n: int, out_count: int) -> list:
+    """`cyclotomic_prefix_ifft` of arrays of n values laid back to back; the
+    first out_count outputs of each."""
+    buf = bytearray(values)
+    count = len(buf) // (GT_BYTES * n)
+    ctx().call("wbte_gt_cyclotomic_prefix_ifft_many", buf, n, out_count, count)
+    return [bytes(buf[GT_BYTES * n * q : GT_BYTES * (n * q + out_count)]) for q in range(count)]
+
+
 def cyclotomic_prefix_ifft(values, out_count: int):
     buf = bytearray(values)
     ctx().call("wbte_gt_cyclotomic_prefix_ifft", buf, len(buf) // GT_BYTES, out_count)
