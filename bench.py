@@ -63,6 +63,60 @@ METRIC = "ciphertexts decrypted/s (weighted_btx batch decryption, B=512)"
 NCU_GT_POWS_DRAM_BYTES = 17.822836e9 + 10.396248e9
 
 
+# Fp products of the tower operations as implemented (Karatsuba Fp2 / Fp6)
+FP12_MUL, CYC_SQR, FROB = 54, 18, 15
+R_FR = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001
+X_ABS = 0xD201000000010000
+
+
+def _plan_cost(s: int) -> int:
+    """Fp products of cyc_pow_plan for the canonical scalar s: the four
+    base-|x| digits in width-4 NAF over one run of squarings, a table of
+    odd powers (1 squaring, 3 products, 12 Frobenius maps)."""
+    longest, nonzero = 0, 0
+    for _ in range(4):
+        v = s % X_ABS
+        s //= X_ABS
+        length = 0
+        while v:
+            d = 0
+            if v & 1:
+                d = v & 15
+                if d >= 8:
+                    d -= 16
+                v -= d
+                nonzero += 1
+            v >>= 1
+            length += 1
+        longest = max(longest, length)
+    return CYC_SQR + 3 * FP12_MUL + 12 * FROB + CYC_SQR * max(0, longest - 1) + FP12_MUL * max(0, nonzero - 1)
+
+
+def gt_prefix_ifft_products(m: int, out_count: int, count: int) -> int:
+    """Fp products of the batched truncated inverse transform as the library
+    runs it for count >= 32 transforms of an even number of radix-4 stages:
+    per stage the warp-uniform-plan twiddle powers (k_gt_radix4_pows_plan)
+    and the butterfly outputs (k_gt_radix4_outputs: four outputs of 3
+    products, two of them with a Frobenius map; two outputs in the last,
+    truncated stage)."""
+    assert out_count == m // 2 and (m.bit_length() - 1) % 2 == 0
+    w_inv = pow(pow(pow(7, (R_FR - 1) >> 32, R_FR), 1 << (32 - (m.bit_length() - 1)), R_FR), R_FR - 2, R_FR)
+    total, h = 0, 1
+    while h < m:
+        blocks = m // (4 * h)
+        for j in range(h):
+            for e in range(3):
+                idx = (2 * j, j, 3 * j)[e] * blocks
+                if idx >= m // 2:
+                    idx -= m // 2
+                if idx:
+                    total += blocks * _plan_cost(pow(w_inv, idx, R_FR))
+        last = 4 * h == m
+        total += (m // 4) * ((2 * 3 * FP12_MUL + FROB) if last else (4 * 3 * FP12_MUL + 2 * FROB))
+        h *= 4
+    return total * count
+
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -451,6 +505,14 @@ def main():
                          "decomposed wNAF plans); the kernels do 25% fewer exponentiations (radix-4) on a "
                          "fixed radix-16 schedule shared by the four digits",
                          "dominant_in_group": top_g[0] == "gt_ifft"})
+        if G >= 32 and G % 32 == 0:
+            own = gt_prefix_ifft_products(m, B, G)
+            roofline.update({"own_fp_products_per_launch_sequence": own,
+                             "own_achieved": own / (gt_ms / 1000.0) / 1e9,
+                             "own_frac": own / (gt_ms / 1000.0) / peak_fp,
+                             "own_basis": "exact count of the Fp products the library's kernels run for this "
+                                          "transform (warp-uniform NAF plans of the twiddles, butterfly outputs); "
+                                          "Fp additions not counted"})
     else:
         roofline.update({"achieved": None, "frac": None})
     group_kernels = {k: {"ms": round(v[0], 2), "launches": v[1]}
