@@ -162,7 +162,11 @@ def test_gt_pow_matches_oracle(orc):
 
 
 @pytest.mark.parametrize("n", [2, 8, 32])
-def test_group_ntt_matches_oracle(orc, n):
+@pytest.mark.parametrize("joint", ["auto", "0", "1"])
+def test_group_ntt_matches_oracle(orc, n, joint, monkeypatch):
+    """The lane-split and the one-thread (joint digit) butterflies."""
+    if joint != "auto":
+        monkeypatch.setenv("WBTE_NTT_JOINT", joint)
     rng = random.Random(300 + n)
     g1 = orc.g1_mul_many(orc.g1_generator(), rs(rng, n, orc.R))
     g2 = orc.g2_mul_many(orc.g2_generator(), rs(rng, n, orc.R))

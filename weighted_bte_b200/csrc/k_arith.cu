@@ -333,6 +333,55 @@ WBTE_INL G1X small_msm_entry(const G1X tab[2][8], int c, int dd) {
     return m;
 }
 
+// [k]v for a canonical scalar k by one thread: all base-|x| digit groups of
+// k (G1: two, G2: four) share one run of doublings (signed radix-16 Straus)
+template <class F>
+static __device__ __noinline__ Xyzz<F> mul_joint(const Xyzz<F> v, const uint8_t* scalar) {
+    using S = SmallMsmDigits<F>;
+    Xyzz<F> tab[S::TABS][8];
+    small_msm_tables(tab, v);
+    uint32_t sc[8];
+    load_scalar(sc, scalar);
+    uint64_t d[4], lo[4], hi[4];
+    decompose_base_x(d, sc);
+    small_msm_digits(lo, hi, d, (const Xyzz<F>*)nullptr);
+    Xyzz<F> acc;
+    set_inf(acc);
+    for (int kk = S::TOP; kk >= 0; kk--) {
+        if (kk != S::TOP) {
+            acc = xyzz_dbl(acc);
+            acc = xyzz_dbl(acc);
+            acc = xyzz_dbl(acc);
+            acc = xyzz_dbl(acc);
+        }
+        for (int c = 0; c < S::D; c++) {
+            const int dd = r16_digit(lo[c], hi[c], kk, S::TOP);
+            if (dd) acc = xyzz_add(acc, small_msm_entry(tab, c, dd));
+        }
+    }
+    return acc;
+}
+
+// One radix-2 butterfly per thread with the twiddle multiplication on one
+// thread (mul_joint: the digit groups share their doublings), for batches of
+// transforms large enough to fill the GPU without the lane split.  Threads
+// take the transforms fastest, so a warp shares one twiddle.
+template <class F>
+__global__ void __launch_bounds__(WARP) k_ntt_stage_joint(uint8_t* work, const uint8_t* tw, int64_t n, int64_t half,
+                                                         int64_t count) {
+    const int64_t g = (int64_t)blockIdx.x * WARP + threadIdx.x;
+    if (g >= (n / 2) * count) return;
+    const int64_t q = g % count, tt = g / count;
+    const int64_t chunk = tt / half, j = tt % half;
+    const int64_t a = q * n + chunk * 2 * half + j, b = a + half;
+    Xyzz<F>* w = reinterpret_cast<Xyzz<F>*>(work);
+    Xyzz<F> t = load_vec(w + b);
+    if (j != 0) t = mul_joint(t, tw + FR_SZ * (j * (n / (2 * half))));
+    const Xyzz<F> u = load_vec(w + a);
+    store_vec(w + a, xyzz_add(u, t));
+    store_vec(w + b, xyzz_add(u, neg(t)));
+}
+
 template <class F>
 __global__ void __launch_bounds__(WARP) k_small_msm(uint8_t* out, const uint8_t* points, const int64_t* pbase,
                                                    const int32_t* idx, const uint8_t* scalars, const int32_t* vsel,
@@ -439,15 +488,21 @@ __global__ void k_g2_compress(uint8_t* out, const uint8_t* in, int64_t n) {
     o[0] |= 0x80 | (largest ? 0x20 : 0);
 }
 
+// [s]G from the generator table (one mixed addition per byte of s) and [c]X
+// by the joint base-|x| form (the two digit groups share their doublings)
 __global__ void k_schnorr_verify(uint8_t* valid, const uint8_t* X, const uint8_t* R, const uint8_t* sresp,
-                                 const uint8_t* c, int64_t n) {
+                                 const uint8_t* c, int64_t n, const uint8_t* gen_table) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    uint32_t ks[8], kc[8];
-    load_scalar(ks, sresp + FR_SZ * i);
-    load_scalar(kc, c + FR_SZ * i);
-    G1X lhs = xyzz_mul(from_affine(g1_generator()), ks);
-    G1X cx = xyzz_mul(from_affine(load_affine(reinterpret_cast<const G1A*>(X + G1_AFF * i))), kc);
+    const G1A* T = reinterpret_cast<const G1A*>(gen_table);
+    const uint8_t* sb = sresp + FR_SZ * i;
+    G1X lhs;
+    set_inf(lhs);
+    for (int w = 0; w < 32; w++) {
+        const uint32_t d = sb[w];
+        if (d) lhs = xyzz_madd(lhs, load_affine(T + 256 * w + d));
+    }
+    G1X cx = mul_joint(from_affine(load_affine(reinterpret_cast<const G1A*>(X + G1_AFF * i))), c + FR_SZ * i);
     G1A r = load_affine(reinterpret_cast<const G1A*>(R + G1_AFF * i));
     G1X rhs = xyzz_madd(cx, r);
     G1X diff = xyzz_add(lhs, neg(rhs));
@@ -567,29 +622,33 @@ void launch_mul_batch(Group g, uint8_t* out, const uint8_t* pts, int64_t stride,
 // on other streams never read a table still being written.
 static uint8_t* g_gen_table[2][64] = {};
 static std::mutex g_gen_mu;
+// the generator table of group g on the current device (null on failure)
+static const uint8_t* generator_table(Group g, cudaStream_t s) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return nullptr;
+    int gi = g == GROUP_G1 ? 0 : 1;
+    size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    std::lock_guard<std::mutex> lock(g_gen_mu);
+    if (!g_gen_table[gi][dev]) {
+        uint8_t* t = nullptr;
+        if (cudaMalloc(&t, aff * 256 * 32) != cudaSuccess) return nullptr;
+        note_launch();
+        if (g == GROUP_G1) k_build_gen_table<Fp><<<32, 256, 0, s>>>(t);
+        else k_build_gen_table<Fp2><<<32, 256, 0, s>>>(t);
+        if (cudaStreamSynchronize(s) != cudaSuccess) return nullptr;
+        g_gen_table[gi][dev] = t;
+    }
+    return g_gen_table[gi][dev];
+}
 void launch_mul_generator(Group g, uint8_t* out, const uint8_t* scalars, int64_t n, cudaStream_t s) {
     ProfScope prof_("mul_generator", s);
     if (n <= 0) return;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) return;
-    int gi = g == GROUP_G1 ? 0 : 1;
-    size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
-    {
-        std::lock_guard<std::mutex> lock(g_gen_mu);
-        if (!g_gen_table[gi][dev]) {
-            uint8_t* t = nullptr;
-            if (cudaMalloc(&t, aff * 256 * 32) != cudaSuccess) return;
-            note_launch();
-            if (g == GROUP_G1) k_build_gen_table<Fp><<<32, 256, 0, s>>>(t);
-            else k_build_gen_table<Fp2><<<32, 256, 0, s>>>(t);
-            if (cudaStreamSynchronize(s) != cudaSuccess) return;
-            g_gen_table[gi][dev] = t;
-        }
-    }
+    const uint8_t* table = generator_table(g, s);
+    if (!table) return;
     note_launch();
-    if (g == GROUP_G1) k_mul_generator<Fp><<<blocks_for(n), TPB, 0, s>>>(out, g_gen_table[gi][dev], scalars, n);
-    else k_mul_generator<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, g_gen_table[gi][dev], scalars, n);
+    if (g == GROUP_G1) k_mul_generator<Fp><<<blocks_for(n), TPB, 0, s>>>(out, table, scalars, n);
+    else k_mul_generator<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, table, scalars, n);
 }
 
 void launch_mul_pow2(Group g, uint8_t* out, const uint8_t* in, int64_t n, int k, cudaStream_t s) {
@@ -613,6 +672,42 @@ void launch_negate(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStre
     else k_negate<Fp2><<<blocks_for(n), TPB, 0, s>>>(out, in, n);
 }
 
+// Whether a transform stage of `butterflies` butterflies runs one thread per
+// butterfly (k_ntt_stage_joint) rather than the lane split: a cost model of one
+// thread's Fp products (G1: 128 doublings and 66 additions joint, against 128
+// and 33 per lane on 2 lanes; G2: 64 and 68 against 64 and 17 per lane on 4
+// lanes) times max(1, threads / resident threads).  WBTE_NTT_JOINT = 0 or 1
+// overrides the choice.
+static bool ntt_joint(Group g, int64_t butterflies) {
+    if (const char* env = getenv("WBTE_NTT_JOINT")) return atoi(env) != 0;
+    static std::atomic<int64_t> cap[2][2] = {{{0}, {0}}, {{0}, {0}}};
+    const int gi = g == GROUP_G1 ? 0 : 1;
+    int64_t c[2];
+    for (int v = 0; v < 2; v++) {
+        c[v] = cap[gi][v].load();
+        if (c[v] == 0) {
+            int dev = 0, sms = 0, blocks = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (g == GROUP_G1)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &blocks, v ? (const void*)k_ntt_stage_joint<Fp> : (const void*)k_ntt_stage<Fp>, WARP, 0);
+            else
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &blocks, v ? (const void*)k_ntt_stage_joint<Fp2> : (const void*)k_ntt_stage<Fp2>, WARP, 0);
+            c[v] = (int64_t)(blocks > 0 ? blocks : 1) * WARP * (sms > 0 ? sms : 1);
+            cap[gi][v].store(c[v]);
+        }
+    }
+    const bool g1 = g == GROUP_G1;
+    const int L = g1 ? NttLanes<Fp>::L : NttLanes<Fp2>::L;
+    const double dbl = g1 ? 9.0 : 30.0, add = g1 ? 12.0 : 42.0, dbls = g1 ? 128.0 : 64.0;
+    const double adds_joint = g1 ? 66.0 + 15.0 : 68.0 + 7.0, adds_lane = g1 ? 33.0 + 8.0 : 17.0 + 7.0;
+    const double joint = std::max(1.0, (double)butterflies / (double)c[1]) * (dbls * dbl + adds_joint * add);
+    const double lane = std::max(1.0, (double)(butterflies * L) / (double)c[0]) * (dbls * dbl + adds_lane * add);
+    return joint < lane;
+}
+
 void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, int64_t n, cudaStream_t s, int64_t count) {
     ProfScope prof_(g == GROUP_G1 ? "ntt_g1" : "ntt_g2", s);
     if (n <= 0 || count <= 0) return;
@@ -622,18 +717,26 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
     if (g == GROUP_G1) {
         note_launch();
         k_ntt_load<Fp><<<blocks_for(total), TPB, 0, s>>>(work, io, n, bits, count);
+        const bool joint = ntt_joint(g, butterflies);
         for (int64_t half = 1; half < n; half *= 2) {
             note_launch();
-            k_ntt_stage<Fp><<<blocks_for(NttLanes<Fp>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
+            if (joint)
+                k_ntt_stage_joint<Fp><<<blocks_for(butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
+            else
+                k_ntt_stage<Fp><<<blocks_for(NttLanes<Fp>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
         }
         note_launch();
         k_xyzz_to_affine<Fp><<<blocks_for(total), TPB, 0, s>>>(io, work, total);
     } else {
         note_launch();
         k_ntt_load<Fp2><<<blocks_for(total), TPB, 0, s>>>(work, io, n, bits, count);
+        const bool joint = ntt_joint(g, butterflies);
         for (int64_t half = 1; half < n; half *= 2) {
             note_launch();
-            k_ntt_stage<Fp2><<<blocks_for(NttLanes<Fp2>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
+            if (joint)
+                k_ntt_stage_joint<Fp2><<<blocks_for(butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
+            else
+                k_ntt_stage<Fp2><<<blocks_for(NttLanes<Fp2>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
         }
         note_launch();
         k_xyzz_to_affine<Fp2><<<blocks_for(total), TPB, 0, s>>>(io, work, total);
@@ -708,7 +811,9 @@ void launch_schnorr_verify(uint8_t* valid, const uint8_t* X, const uint8_t* R, c
     ProfScope prof_("schnorr_verify", st);
     if (n <= 0) return;
     note_launch();
-    k_schnorr_verify<<<blocks_for(n), TPB, 0, st>>>(valid, X, R, sresp, c, n);
+    const uint8_t* table = generator_table(GROUP_G1, st);
+    if (!table) return;
+    k_schnorr_verify<<<blocks_for(n), TPB, 0, st>>>(valid, X, R, sresp, c, n, table);
 }
 
 }  // namespace wbte
