@@ -16,6 +16,17 @@ inline unsigned blocks_for(int64_t n, int tpb = TPB) { return (unsigned)((n + tp
 WBTE_INL Fp12* as_gt(uint8_t* p) { return reinterpret_cast<Fp12*>(p); }
 WBTE_INL const Fp12* as_gt(const uint8_t* p) { return reinterpret_cast<const Fp12*>(p); }
 
+// resident 64-thread blocks per SM the Miller-loop and final-exponentiation
+// kernels are compiled for (0: no bound, the compiler's 255 registers)
+#ifndef WBTE_PAIR_MINBLOCKS
+#define WBTE_PAIR_MINBLOCKS 0
+#endif
+#if WBTE_PAIR_MINBLOCKS > 0
+#define WBTE_PAIR_BOUNDS __launch_bounds__(TPB, WBTE_PAIR_MINBLOCKS)
+#else
+#define WBTE_PAIR_BOUNDS
+#endif
+
 __global__ void k_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -36,7 +47,7 @@ __global__ void k_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n) {
 }
 
 // pair i uses line table i % lines_n (tables stored line-major, stride lines_n)
-__global__ void k_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t lines_n) {
+__global__ void WBTE_PAIR_BOUNDS k_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t lines_n) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     G1A P = load_affine(reinterpret_cast<const G1A*>(p + G1_AFF * i));
@@ -48,7 +59,7 @@ __global__ void k_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t
 // out[o] = prod_{t < T} Miller(P[(o / per) * T + t], lines of table (o % per) * T + t):
 // the opening of K batches against one committee's prepared opening keys
 // (tables line-major with stride per * T), each batch with its own T shares.
-__global__ void k_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per,
+__global__ void WBTE_PAIR_BOUNDS k_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per,
                                      int T) {
     int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (o >= n) return;
@@ -59,7 +70,7 @@ __global__ void k_miller_lines_multi(uint8_t* out, const uint8_t* lines, const u
     store_vec(as_gt(out) + o, f);
 }
 
-__global__ void k_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, int64_t p_mod, int64_t q_mod) {
+__global__ void WBTE_PAIR_BOUNDS k_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, int64_t p_mod, int64_t q_mod) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     G1A P = load_affine(reinterpret_cast<const G1A*>(p + G1_AFF * (p_mod ? i % p_mod : i)));
@@ -80,7 +91,7 @@ __global__ void k_fp12_segment_product(uint8_t* out, const uint8_t* in, const in
     store_vec(as_gt(out) + j, acc);
 }
 
-__global__ void k_final_exp(uint8_t* out, const uint8_t* in, int64_t n, int mode) {
+__global__ void WBTE_PAIR_BOUNDS k_final_exp(uint8_t* out, const uint8_t* in, int64_t n, int mode) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     Fp12 f = load_vec(as_gt(in) + i), r;
@@ -114,6 +125,11 @@ constexpr int WARP = 32;
 // resident blocks per SM the GT kernels are compiled for (register budget)
 #ifndef WBTE_GT_MINBLOCKS
 #define WBTE_GT_MINBLOCKS 1
+#endif
+// k_gt_radix4_pows_plan: 12 one-warp blocks per SM (170 registers) hide more
+// latency than 8 blocks at 255 registers, in spite of the spills
+#ifndef WBTE_PLAN_MINBLOCKS
+#define WBTE_PLAN_MINBLOCKS 12
 #endif
 
 // parts of v^s for the butterfly or element this lane belongs to
@@ -296,7 +312,7 @@ __global__ void __launch_bounds__(WARP, WBTE_GT_MINBLOCKS) k_gt_radix4_pows(uint
 // cyc_pow_plan) runs without divergence: about 4.3 k Fp products per power
 // against 5.8 k for the fixed radix-16 schedule.  Same ex layout as
 // k_gt_radix4_pows.
-__global__ void __launch_bounds__(WARP, WBTE_GT_MINBLOCKS) k_gt_radix4_pows_plan(uint8_t* ex, const uint8_t* io,
+__global__ void __launch_bounds__(WARP, WBTE_PLAN_MINBLOCKS) k_gt_radix4_pows_plan(uint8_t* ex, const uint8_t* io,
                                                              const uint8_t* tw, int64_t n, int64_t h,
                                                              int64_t count) {
     const int64_t g = (int64_t)blockIdx.x * WARP + threadIdx.x;
