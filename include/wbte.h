@@ -281,6 +281,19 @@ int32_t wbte_wbtx_precompute_many(wbte_ctx *ctx, void *beta, const void *kernel_
 int32_t wbte_wbtx_open_many(wbte_ctx *ctx, void *messages, const void *opening_keys, const void *opening_lines,
                             const void *sigma, uint64_t T, const void *second, const void *beta,
                             const uint8_t *valid, uint64_t batch_size, uint64_t K);
+/* Precompute and open in one call for K batches of one committee (the
+ * batched form of decrypt(), weighted_btx/src/decryption.rs:555-695):
+ * messages K*B GT, at valid slots second * beta / alpha, one elsewhere.  The
+ * cross terms and the opening pairings meet before the hard part of the
+ * final exponentiation, which is a fixed power (a homomorphism of the
+ * cyclotomic subgroup), so each slot takes one hard part instead of two;
+ * the messages equal precompute_many followed by open_many.  Arguments as
+ * there: kernel_lines m tables, opening_keys B*T G2 and opening_lines (or
+ * NULL), first K*B G1, second K*B GT, valid K*B, sigma K*T G1. */
+int32_t wbte_wbtx_decrypt_many(wbte_ctx *ctx, void *messages, const void *kernel_lines, const void *opening_keys,
+                               const void *opening_lines, const void *first, const void *second,
+                               const uint8_t *valid, const void *sigma, uint64_t T, uint64_t batch_size,
+                               uint64_t K);
 /* Public key material of keygen_with_rng (weighted_btx/src/setup.rs:98-233):
  *   verification_keys[i * N + j] = [q_pos[i * N + j]] G2            (i < L)
  *   negative[i * W + w]          = [z[w] q_neg[i * N + owner[w]]] G2 (i < L)

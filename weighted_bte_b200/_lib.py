@@ -142,6 +142,7 @@ _SIGNATURES = {
     "wbte_wbtx_verify_shares_many": [_VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64, _U64],
     "wbte_wbtx_precompute_many": [_VP, _VP, _VP, _VP, _U64, _U64],
     "wbte_wbtx_open_many": [_VP, _VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64, _U64],
+    "wbte_wbtx_decrypt_many": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64, _U64],
     "wbte_pfe_kernel": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
     "wbte_pfe_precompute": [_VP, _VP, _VP, _VP, _VP, _U64],
     "wbte_pfe_open": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64],

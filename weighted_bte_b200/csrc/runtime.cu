@@ -1776,6 +1776,35 @@ int32_t wbte_wbtx_precompute_many(wbte_ctx* ctx, void* beta, const void* kernel_
     return c.finish();
 }
 
+// alpha[b B + i] = prod_t Miller(sigma[b T + t], opening_keys[i T + t]) before
+// the final exponentiation (weighted_btx/src/decryption.rs:607-695): one
+// multi-Miller loop per slot over the prepared opening keys when their line
+// tables are given (T <= 8), else T unprepared loops and their product
+static bool opening_miller(Call& c, uint8_t* alpha, const uint8_t* dk, const void* opening_lines, const uint8_t* ds,
+                           uint64_t T, uint64_t B, uint64_t K) {
+    const uint64_t BT = B * T;
+    if (opening_lines && T <= 8) {
+        const uint8_t* dl = c.in(opening_lines, LINE_SZ * LINES_PER_POINT * BT);
+        if (!c.ok()) return false;
+        launch_miller_lines_multi(alpha, dl, ds, (int64_t)(B * K), (int64_t)B, (int)T, c.s);
+        return true;
+    }
+    uint8_t* P = c.alloc(G1_AFF * BT * K);
+    uint8_t* f = c.alloc(GT_SZ * BT * K);
+    std::vector<int32_t> pidx(BT * K);
+    for (uint64_t b = 0; b < K; b++)
+        for (uint64_t x = 0; x < BT; x++) pidx[b * BT + x] = (int32_t)(b * T + x % T);
+    std::vector<int64_t> offs(B * K + 1);
+    for (uint64_t i = 0; i <= B * K; i++) offs[i] = (int64_t)(i * T);
+    const int32_t* dpidx = c.in_vec(pidx);
+    const int64_t* doffs = c.in_vec(offs);
+    if (!c.ok()) return false;
+    launch_gather(P, ds, dpidx, (int64_t)(BT * K), G1_AFF, c.s);
+    launch_miller(f, P, dk, (int64_t)(BT * K), c.s, 0, (int64_t)BT);
+    launch_fp12_segment_product(alpha, f, doffs, (int64_t)(B * K), c.s);
+    return true;
+}
+
 int32_t wbte_wbtx_open_many(wbte_ctx* ctx, void* messages, const void* opening_keys, const void* opening_lines,
                             const void* sigma, uint64_t T, const void* second, const void* beta, const uint8_t* valid,
                             uint64_t B, uint64_t K) {
@@ -1789,34 +1818,55 @@ int32_t wbte_wbtx_open_many(wbte_ctx* ctx, void* messages, const void* opening_k
     const uint8_t* d2 = c.in(second, GT_SZ * B * K);
     const uint8_t* db = c.in(beta, GT_SZ * B * K);
     const uint8_t* dv = c.in(valid, B * K);
-    const uint64_t BT = B * T;
     uint8_t* alpha = c.alloc(GT_SZ * B * K);
-    if (opening_lines && T <= 8) {
-        // prepared opening keys: one multi-Miller loop per slot shares the
-        // squarings across the T shares
-        const uint8_t* dl = c.in(opening_lines, LINE_SZ * LINES_PER_POINT * BT);
-        if (!c.ok()) return c.finish();
-        launch_miller_lines_multi(alpha, dl, ds, (int64_t)(B * K), (int64_t)B, (int)T, c.s);
-        launch_final_exp(alpha, alpha, (int64_t)(B * K), FE_FULL, c.s);
-        launch_unmask(dm, d2, alpha, db, dv, (int64_t)(B * K), c.s);
-        return c.finish();
-    }
-    uint8_t* P = c.alloc(G1_AFF * BT * K);
-    uint8_t* f = c.alloc(GT_SZ * BT * K);
-    std::vector<int32_t> pidx(BT * K);
-    for (uint64_t b = 0; b < K; b++)
-        for (uint64_t x = 0; x < BT; x++) pidx[b * BT + x] = (int32_t)(b * T + x % T);
-    std::vector<int64_t> offs(B * K + 1);
-    for (uint64_t i = 0; i <= B * K; i++) offs[i] = (int64_t)(i * T);
-    const int32_t* dpidx = c.in_vec(pidx);
-    const int64_t* doffs = c.in_vec(offs);
-    if (!c.ok()) return c.finish();
-    // alpha[b B + i] = prod_k e(sigma[b T + k], opening_keys[i T + k]) (weighted_btx/src/decryption.rs:607-695)
-    launch_gather(P, ds, dpidx, (int64_t)(BT * K), G1_AFF, c.s);
-    launch_miller(f, P, dk, (int64_t)(BT * K), c.s, 0, (int64_t)BT);
-    launch_fp12_segment_product(alpha, f, doffs, (int64_t)(B * K), c.s);
+    if (!c.ok() || !opening_miller(c, alpha, dk, opening_lines, ds, T, B, K)) return c.finish();
     launch_final_exp(alpha, alpha, (int64_t)(B * K), FE_FULL, c.s);
     launch_unmask(dm, d2, alpha, db, dv, (int64_t)(B * K), c.s);
+    return c.finish();
+}
+
+int32_t wbte_wbtx_decrypt_many(wbte_ctx* ctx, void* messages, const void* kernel_lines, const void* opening_keys,
+                               const void* opening_lines, const void* first, const void* second, const uint8_t* valid,
+                               const void* sigma, uint64_t T, uint64_t B, uint64_t K) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!messages || !kernel_lines || !opening_keys || !first || !second || !valid || !sigma || B == 0 || T == 0 ||
+        K == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    const uint64_t m = next_pow2(2 * B), n = B * K;
+    uint8_t* dm = c.out(messages, GT_SZ * n);
+    const uint8_t* dl = c.in(kernel_lines, LINE_SZ * LINES_PER_POINT * m);
+    const uint8_t* dk = c.in(opening_keys, G2_AFF * B * T);
+    const uint8_t* dfirst = c.in(first, G1_AFF * n);
+    const uint8_t* d2 = c.in(second, GT_SZ * n);
+    const uint8_t* dv = c.in(valid, n);
+    const uint8_t* ds = c.in(sigma, G1_AFF * T * K);
+    uint8_t* x = c.zeros(G1_AFF * m * K);
+    uint8_t* work = c.alloc(G1_XYZZ * m * K);
+    uint8_t* f = c.alloc(GT_SZ * m * K);
+    uint8_t* y = c.alloc(GT_SZ * n);
+    uint8_t* alpha = c.alloc(GT_SZ * n);
+    const uint8_t* tw = twiddles(c, (int64_t)m, false);
+    const uint8_t* twi = twiddles(c, (int64_t)m, true);
+    if (!c.ok()) return c.finish();
+    // the cross terms up to the truncated cyclotomic transform, as precompute
+    cudaMemcpy2DAsync(x, G1_AFF * m, dfirst, G1_AFF * B, G1_AFF * B, K, cudaMemcpyDeviceToDevice, c.s);
+    launch_group_ntt(GROUP_G1, x, work, tw, (int64_t)m, c.s, (int64_t)K);
+    launch_miller_lines(f, dl, x, (int64_t)(m * K), c.s, (int64_t)m);
+    launch_final_exp(f, f, (int64_t)(m * K), FE_EASY, c.s);
+    launch_cyclotomic_prefix_ifft(f, twi, (int64_t)m, (int64_t)B, c.s, (int64_t)K);
+    // the opening's pairings up to their easy part
+    if (!opening_miller(c, alpha, dk, opening_lines, ds, T, B, K)) return c.finish();
+    launch_final_exp(alpha, alpha, (int64_t)n, FE_EASY, c.s);
+    // beta / alpha = hard(t) / hard(easy(a)) = hard(t conj(easy(a))): the hard
+    // part is a fixed power, a homomorphism of the cyclotomic subgroup, where
+    // conjugation is the inverse; one hard part per slot instead of two
+    cudaMemcpy2DAsync(y, GT_SZ * B, f, GT_SZ * m, GT_SZ * B, K, cudaMemcpyDeviceToDevice, c.s);
+    launch_fp12_mul(y, y, 1, alpha, 1, true, (int64_t)n, c.s);
+    launch_final_exp(y, y, (int64_t)n, FE_HARD, c.s);
+    // messages = second beta / alpha at valid slots, one elsewhere
+    launch_fp12_mul(dm, d2, 1, y, 1, false, (int64_t)n, c.s);
+    launch_fp12_mask(dm, dv, (int64_t)n, c.s);
     return c.finish();
 }
 

@@ -218,12 +218,13 @@ def decrypt_group(dk: wb.PublicDecryptionKey, batches: Sequence, party_keys: Seq
     pre = cache.get(dk, accepted[0]) if cache is not None else wb.prepare_decryption(dk, accepted[0])
     Ta = accepted[0].party_count()
     sigmas = b"".join(s.sigma for a in accepted for s in a.shares())
-    beta = wb.empty_device(GTB * B * K)
-    ctx.call("wbte_wbtx_precompute_many", beta, pre.kernel_lines, first, valid, B, K)
     second = torch.cat([c.second[: GTB * B] if isinstance(c, wb.CiphertextBatch)
                         else wb.to_device(b"".join(x.second for x in c)) for c in batches])
     out = wb.empty_device(GTB * B * K)
-    ctx.call("wbte_wbtx_open_many", out, pre.opening_keys, pre.opening_lines, sigmas, Ta, second, beta, valid, B, K)
+    # precompute_batch and open_batch of all K batches, the cross terms and the
+    # opening pairings sharing one hard final exponentiation per slot
+    ctx.call("wbte_wbtx_decrypt_many", out, pre.kernel_lines, pre.opening_keys, pre.opening_lines, first, second,
+             valid, sigmas, Ta, B, K)
     if device_output:
         return [out[GTB * B * b : GTB * B * (b + 1)] for b in range(K)]
     host = wb.to_host(out, GTB * B * K)
