@@ -8,6 +8,9 @@ seeded synthetic inputs with the shapes of the benchmark configurations.
   a set is authorized when its weight exceeds t = floor(W / 3); the
   committee is the heaviest-first minimal authorized set
   (weighted_btx/examples/paper_reproduction.rs:581-607); ChaCha20 seed 1.
+* weighted_pfe served form: n = 1000 parties with Pareto(1.2) weights
+  scaled to W = 16384; batched form: n = 64 parties with Zipf(1) weights
+  scaled to W = 2048; threshold floor(W / 3).
 * Plaintexts are uniform 32-byte strings mapped to GT as
   Gt::generator()^(LE(bytes) mod r); the crates encrypt GT elements only.
 """
@@ -39,6 +42,38 @@ def zipf_weights(n: int, total: int, s: float = 1.0) -> List[int]:
         base[j] -= 1
         rest += 1
     return base
+
+
+def scale_weights(raw: List[float], total: int) -> List[int]:
+    """Largest-remainder integer weights proportional to `raw`, each >= 1,
+    summing to `total`."""
+    n = len(raw)
+    if total < n:
+        raise ValueError("total weight must be at least the party count")
+    norm = sum(raw)
+    quotas = [r * total / norm for r in raw]
+    base = [max(1, int(q)) for q in quotas]
+    rest = total - sum(base)
+    order = sorted(range(n), key=lambda i: (-(quotas[i] - int(quotas[i])), i))
+    i = 0
+    while rest > 0:
+        base[order[i % n]] += 1
+        rest -= 1
+        i += 1
+    while rest < 0:
+        j = max(range(n), key=lambda k: (base[k], -k))
+        base[j] -= 1
+        rest += 1
+    return base
+
+
+def pareto_weights(n: int, total: int, alpha: float = 1.2, seed: int = 4) -> List[int]:
+    """Heavy-tailed integer weights: n seeded Pareto(alpha) draws
+    (1 - U)^(-1/alpha), scaled to `total` (each >= 1)."""
+    import random
+
+    rng = random.Random(seed)
+    return scale_weights([(1.0 - rng.random()) ** (-1.0 / alpha) for _ in range(n)], total)
 
 
 def minimal_authorized_parties(weights: List[int], threshold: int) -> Tuple[List[int], int]:
