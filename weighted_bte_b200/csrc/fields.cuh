@@ -34,8 +34,16 @@ WBTE_INL Fp fp_sqr(const Fp& a) { return fp_mul_ool(a, a); }
 WBTE_INL Fp fp_mul(const Fp& a, const Fp& b) { Fp r; fp_mont_mul(r.v, a.v, b.v); return r; }
 WBTE_INL Fp fp_sqr(const Fp& a) { Fp r; fp_mont_mul(r.v, a.v, a.v); return r; }
 #endif
+#if defined(WBTE_FPADD_NOINLINE)
+// out-of-line sums: smaller code for kernels bound by instruction fetch
+static __device__ __noinline__ Fp fp_add_ool(Fp a, Fp b) { Fp r; fp_add_raw(r.v, a.v, b.v); return r; }
+static __device__ __noinline__ Fp fp_sub_ool(Fp a, Fp b) { Fp r; fp_sub_raw(r.v, a.v, b.v); return r; }
+WBTE_INL Fp fp_add(const Fp& a, const Fp& b) { return fp_add_ool(a, b); }
+WBTE_INL Fp fp_sub(const Fp& a, const Fp& b) { return fp_sub_ool(a, b); }
+#else
 WBTE_INL Fp fp_add(const Fp& a, const Fp& b) { Fp r; fp_add_raw(r.v, a.v, b.v); return r; }
 WBTE_INL Fp fp_sub(const Fp& a, const Fp& b) { Fp r; fp_sub_raw(r.v, a.v, b.v); return r; }
+#endif
 // a + b without reduction: only valid as a multiplication input (< 2p).
 WBTE_INL Fp fp_add_lazy(const Fp& a, const Fp& b) { Fp r; fp_add_nored(r.v, a.v, b.v); return r; }
 WBTE_INL Fp fp_dbl(const Fp& a) { return fp_add(a, a); }
