@@ -58,9 +58,10 @@ FP_MULS_PER_G2_MADD = 8 * 3 + 2 * 2
 METRIC = "ciphertexts decrypted/s (weighted_btx batch decryption, B=512)"
 
 
-# DRAM bytes (read + write) of one k_gt_radix4_pows<1> launch at this workload
-# (second radix-4 stage, 64 transforms of m = 1024), from one ncu capture
-NCU_GT_POWS_DRAM_BYTES = 17.822836e9 + 10.396248e9
+# DRAM bytes (read + write) of one k_gt_radix4_pows_plan launch at this
+# workload (second radix-4 stage, 64 transforms of m = 1024), from one ncu
+# capture
+NCU_GT_PLAN_DRAM_BYTES = 7.531103e9 + 20.206864e9
 
 
 # Fp products of the tower operations as implemented (Karatsuba Fp2 / Fp6)
@@ -485,13 +486,13 @@ def main():
     top_g = max(prof_g.items(), key=lambda kv: kv[1][0])
     gt_ms = prof_g.get("gt_ifft", (0.0, 0))[0]
     m = wb.transform_size_for(B)
-    roofline = {"kernel": "gt_ifft (truncated cyclotomic inverse transform, batched form: k_gt_radix4_pows + "
+    roofline = {"kernel": "gt_ifft (truncated cyclotomic inverse transform, batched form: k_gt_radix4_pows_plan + "
                           "k_gt_radix4_outputs per radix-4 stage)",
                 "bound": "int", "unit": "G Fp products/s",
                 "peak_basis": f"measured {float(rate[0]) / 1e12:.2f} T IMAD/s (calibration kernel, mad.lo/mad.hi "
                               f"mix) / {IMAD_PER_FP_MUL} IMAD per Fp product",
-                "traffic": NCU_GT_POWS_DRAM_BYTES if G == 64 and B == 512 else None,
-                "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one k_gt_radix4_pows<1> launch "
+                "traffic": NCU_GT_PLAN_DRAM_BYTES if G == 64 and B == 512 else None,
+                "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one k_gt_radix4_pows_plan launch "
                                  "(radix-4 stage h=16 of 64 transforms, m=1024) from one ncu capture of this "
                                  "workload; the per-thread stack (tables, spills), against 2 x 576 B of "
                                  "algorithmic input and output per exponentiation",
