@@ -491,9 +491,11 @@ def main():
                 "bound": "int", "unit": "G Fp products/s",
                 "peak_basis": f"measured {float(rate[0]) / 1e12:.2f} T IMAD/s (calibration kernel, mad.lo/mad.hi "
                               f"mix) / {IMAD_PER_FP_MUL} IMAD per Fp product",
-                "traffic": NCU_GT_PLAN_DRAM_BYTES if G == 64 and B == 512 else None,
+                "traffic": NCU_GT_PLAN_DRAM_BYTES * G / 64 if G % 32 == 0 and B == 512 else None,
                 "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one k_gt_radix4_pows_plan launch "
                                  "(radix-4 stage h=16 of 64 transforms, m=1024) from one ncu capture of this "
+                                 "workload at 64 batches per group, scaled by G/64 (the traffic is per-thread "
+                                 "stack, proportional to the powers of the launch); "
                                  "workload; the per-thread stack (tables, spills), against 2 x 576 B of "
                                  "algorithmic input and output per exponentiation",
                 "peak": peak_fp / 1e9}
