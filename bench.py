@@ -495,8 +495,7 @@ def main():
                 "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of one k_gt_radix4_pows_plan launch "
                                  "(radix-4 stage h=16 of 64 transforms, m=1024) from one ncu capture of this "
                                  "workload at 64 batches per group, scaled by G/64 (the traffic is per-thread "
-                                 "stack, proportional to the powers of the launch); "
-                                 "workload; the per-thread stack (tables, spills), against 2 x 576 B of "
+                                 "stack, proportional to the powers of the launch): the tables and spills, against 2 x 576 B of "
                                  "algorithmic input and output per exponentiation",
                 "peak": peak_fp / 1e9}
     if gt_ms > 0 and m == work["cyclotomic_prefix_ifft"]["m"] and B == work["cyclotomic_prefix_ifft"]["outputs"]:
