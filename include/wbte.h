@@ -138,6 +138,19 @@ int32_t wbte_g2_sum(wbte_ctx *ctx, void *out, const void *in, const int64_t *off
 /* ZCash compressed encodings, 48 / 96 bytes per point (to_compressed). */
 int32_t wbte_g1_compress(wbte_ctx *ctx, void *out, const void *in, uint64_t n);
 int32_t wbte_g2_compress(wbte_ctx *ctx, void *out, const void *in, uint64_t n);
+/* Decoding of compressed points, as blstrs' checked G1Affine / G2Affine
+ * ::from_compressed used when the crates deserialize keys and ciphertexts
+ * (serde of the key material, weighted_btx/src/setup.rs:21-61; the wire sizes
+ * of weighted_pfe/README.md:159-214): ZCash flags (0x80 compressed, 0x40
+ * infinity, 0x20 larger y), canonical x, y from the curve equation, and when
+ * check_group is nonzero [r]P = O.  n points of 48 (G1) or 96 (G2) bytes in,
+ * affine points out; status (n bytes, may be NULL) per point: 0 ok, 1 bad
+ * encoding, 2 not on the curve, 3 not in the subgroup, the point then written
+ * as the identity.  Returns WBTE_ERR_NOT_ON_CURVE if any point was rejected. */
+int32_t wbte_g1_decompress(wbte_ctx *ctx, void *out, uint8_t *status, const void *in, uint64_t n,
+                           int32_t check_group);
+int32_t wbte_g2_decompress(wbte_ctx *ctx, void *out, uint8_t *status, const void *in, uint64_t n,
+                           int32_t check_group);
 
 /* ------------------------------------------------------- transforms */
 /* In-place radix-2 transform of n affine points over the size-n subgroup of

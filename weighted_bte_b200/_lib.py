@@ -118,6 +118,8 @@ _SIGNATURES = {
     "wbte_lagrange_at_zero": [_VP, _VP, _U64],
     "wbte_schnorr_verify": [_VP, _VP, _VP, _VP, _VP, _U64],
     "wbte_transcript_challenges": [_VP, _VP, ctypes.c_uint32, _U64],
+    "wbte_g1_decompress": [_VP, _VP, _VP, _U64, _I32],
+    "wbte_g2_decompress": [_VP, _VP, _VP, _U64, _I32],
     "wbte_wbtx_partial_decrypt": [_VP, _VP, _U64, _VP, _U64],
     "wbte_wbtx_verify_shares": [_VP, _VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64],
     "wbte_wbtx_prepare": [_VP, _VP, _U64, _U64, _VP, _VP, _VP],

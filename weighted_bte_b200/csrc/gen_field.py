@@ -298,6 +298,11 @@ def gen_constants():
         "0x%08xu" % l for l in limbs32((P - 1) // 2, 12)))
     w("__device__ __constant__ const uint32_t C_P_MINUS_2[12] = {%s};" % ", ".join(
         "0x%08xu" % l for l in limbs32(P - 2, 12)))
+    w("// square-root exponents: (p + 1) / 4 in Fp, (p - 3) / 4 in Fp2 (p = 3 mod 4)")
+    w("__device__ __constant__ const uint32_t C_P_PLUS1_DIV4[12] = {%s};" % ", ".join(
+        "0x%08xu" % l for l in limbs32((P + 1) // 4, 12)))
+    w("__device__ __constant__ const uint32_t C_P_MINUS3_DIV4[12] = {%s};" % ", ".join(
+        "0x%08xu" % l for l in limbs32((P - 3) // 4, 12)))
     w("__device__ __constant__ const uint32_t C_R_MINUS_2[8] = {%s};" % ", ".join(
         "0x%08xu" % l for l in limbs32(R - 2, 8)))
     # Radix-2 domain generators: the two-adic root 7^((r-1)/2^32), squared down.

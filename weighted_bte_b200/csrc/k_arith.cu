@@ -488,6 +488,162 @@ __global__ void k_g2_compress(uint8_t* out, const uint8_t* in, int64_t n) {
     o[0] |= 0x80 | (largest ? 0x20 : 0);
 }
 
+// ------------------------------------------------------- decompression
+// ZCash-format decoding as blstrs' checked from_compressed: big-endian x with
+// flags in the top bits of the first byte (0x80 compressed, 0x40 infinity,
+// 0x20 y is the larger root); x must be canonical, the point on the curve and,
+// when asked, in the prime-order subgroup ([r]P = O).
+enum DecodeStatus : uint8_t { DECODE_OK = 0, DECODE_BAD_ENCODING = 1, DECODE_NOT_ON_CURVE = 2, DECODE_NOT_IN_GROUP = 3 };
+
+// a^e for one of the square-root exponents (E = 0: (p + 1) / 4, 1: (p - 3) / 4),
+// 4-bit fixed windows; F = Fp or Fp2
+template <int E, class F>
+static __device__ __noinline__ F pow_sqrt_exp(F a) {
+    F tab[16];
+    f_set_one(tab[0]);
+    tab[1] = a;
+    for (int i = 2; i < 16; i++) tab[i] = f_mul(tab[i - 1], a);
+    F r;
+    f_set_one(r);
+    bool started = false;
+    for (int w = 95; w >= 0; w--) {
+        if (started) {
+            r = f_sqr(r);
+            r = f_sqr(r);
+            r = f_sqr(r);
+            r = f_sqr(r);
+        }
+        const uint32_t limb = E == 0 ? C_P_PLUS1_DIV4[w / 8] : C_P_MINUS3_DIV4[w / 8];
+        const uint32_t d = (limb >> (4 * (w % 8))) & 15u;
+        if (d) {
+            r = started ? f_mul(r, tab[d]) : tab[d];
+            started = true;
+        }
+    }
+    return r;
+}
+
+// big-endian 48 bytes -> canonical limbs; false if the value is not below p
+WBTE_INL bool fp_load_be48(Fp& canon, const uint8_t* in, uint8_t first_mask) {
+    for (int i = 0; i < 12; i++) canon.v[i] = 0;
+    for (int b = 0; b < 48; b++) {
+        const uint32_t byte = b == 0 ? (in[0] & first_mask) : in[b];
+        canon.v[(47 - b) >> 2] |= byte << (8 * ((47 - b) & 3));
+    }
+    for (int i = 11; i >= 0; i--)
+        if (canon.v[i] != C_P[i]) return canon.v[i] < C_P[i];
+    return false;
+}
+
+// sqrt in Fp (p = 3 mod 4): a^((p + 1) / 4), checked
+WBTE_INL bool fp_sqrt(Fp& r, const Fp& a) {
+    r = pow_sqrt_exp<0>(a);
+    return fp_eq(fp_sqr(r), a);
+}
+
+// sqrt in Fp2 for p = 3 mod 4, the complex method (Adj and Rodriguez-
+// Henriquez, "Square root computation over even extension fields",
+// Algorithm 9): a1 = a^((p - 3) / 4), alpha = a1^2 a, x0 = a1 a; alpha = -1
+// gives u x0, else (1 + alpha)^((p - 1) / 2) x0; the result is checked
+WBTE_INL bool fp2_sqrt(Fp2& r, const Fp2& a) {
+    const Fp2 a1 = pow_sqrt_exp<1>(a);
+    const Fp2 alpha = fp2_mul(fp2_sqr(a1), a);
+    const Fp2 x0 = fp2_mul(a1, a);
+    const Fp2 minus_one = fp2_neg(fp2_one());
+    if (fp2_eq(alpha, minus_one)) {
+        r = Fp2{fp_neg(x0.c1), x0.c0};  // u x0
+    } else {
+        // (1 + alpha)^((p - 1) / 2) = (1 + alpha)^((p - 3) / 4 * 2 + 1)
+        const Fp2 t = fp2_add(fp2_one(), alpha);
+        const Fp2 h = pow_sqrt_exp<1>(t);
+        r = fp2_mul(fp2_mul(fp2_sqr(h), t), x0);
+    }
+    return fp2_eq(fp2_sqr(r), a);
+}
+
+template <class F>
+WBTE_INL bool in_prime_subgroup(const Affine<F>& p) {
+    uint32_t r[8];
+    for (int i = 0; i < 8; i++) r[i] = C_R[i];
+    return is_inf(xyzz_mul(from_affine(p), r));
+}
+
+__global__ void k_g1_decompress(uint8_t* out, uint8_t* status, const uint8_t* in, int64_t n, int check_group) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint8_t* c = in + 48 * i;
+    G1A p;
+    set_inf(p);
+    uint8_t st = DECODE_OK;
+    const uint8_t flags = c[0] & 0xe0;
+    if (!(flags & 0x80)) {
+        st = DECODE_BAD_ENCODING;
+    } else if (flags & 0x40) {
+        bool zero = (flags & 0x20) == 0 && (c[0] & 0x1f) == 0;
+        for (int b = 1; b < 48; b++) zero = zero && c[b] == 0;
+        if (!zero) st = DECODE_BAD_ENCODING;
+    } else {
+        Fp x;
+        if (!fp_load_be48(x, c, 0x1f)) {
+            st = DECODE_BAD_ENCODING;
+        } else {
+            x = fp_to_mont(x);
+            const Fp rhs = fp_add(fp_mul(fp_sqr(x), x), fp_from_const(C_FP_B1));
+            Fp y;
+            if (!fp_sqrt(y, rhs)) {
+                st = DECODE_NOT_ON_CURVE;
+            } else {
+                if (fp_largest(y) != ((flags & 0x20) != 0)) y = fp_neg(y);
+                p.x = x;
+                p.y = y;
+                if (check_group && !in_prime_subgroup(p)) st = DECODE_NOT_IN_GROUP;
+            }
+        }
+    }
+    if (st != DECODE_OK) set_inf(p);
+    store_affine(reinterpret_cast<G1A*>(out + G1_AFF * i), p);
+    status[i] = st;
+}
+
+__global__ void k_g2_decompress(uint8_t* out, uint8_t* status, const uint8_t* in, int64_t n, int check_group) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint8_t* c = in + 96 * i;
+    G2A p;
+    set_inf(p);
+    uint8_t st = DECODE_OK;
+    const uint8_t flags = c[0] & 0xe0;
+    if (!(flags & 0x80)) {
+        st = DECODE_BAD_ENCODING;
+    } else if (flags & 0x40) {
+        bool zero = (flags & 0x20) == 0 && (c[0] & 0x1f) == 0;
+        for (int b = 1; b < 96; b++) zero = zero && c[b] == 0;
+        if (!zero) st = DECODE_BAD_ENCODING;
+    } else {
+        Fp x1, x0;  // x = x0 + x1 u, x1 first
+        if (!fp_load_be48(x1, c, 0x1f) || !fp_load_be48(x0, c + 48, 0xff)) {
+            st = DECODE_BAD_ENCODING;
+        } else {
+            const Fp2 x{fp_to_mont(x0), fp_to_mont(x1)};
+            const Fp2 b{fp_from_const(C_FP_B1), fp_from_const(C_FP_B1)};  // 4 (1 + u)
+            const Fp2 rhs = fp2_add(fp2_mul(fp2_sqr(x), x), b);
+            Fp2 y;
+            if (!fp2_sqrt(y, rhs)) {
+                st = DECODE_NOT_ON_CURVE;
+            } else {
+                const bool largest = fp_is_zero(y.c1) ? fp_largest(y.c0) : fp_largest(y.c1);
+                if (largest != ((flags & 0x20) != 0)) y = fp2_neg(y);
+                p.x = x;
+                p.y = y;
+                if (check_group && !in_prime_subgroup(p)) st = DECODE_NOT_IN_GROUP;
+            }
+        }
+    }
+    if (st != DECODE_OK) set_inf(p);
+    store_affine(reinterpret_cast<G2A*>(out + G2_AFF * i), p);
+    status[i] = st;
+}
+
 // [s]G from the generator table (one mixed addition per byte of s) and [c]X
 // by the joint base-|x| form (the two digit groups share their doublings)
 __global__ void k_schnorr_verify(uint8_t* valid, const uint8_t* X, const uint8_t* R, const uint8_t* sresp,
@@ -796,6 +952,15 @@ void launch_small_msm(Group g, uint8_t* out, const uint8_t* points, const int64_
         k_small_msm<Fp><<<blocks_for(L * k, WARP), WARP, 0, s>>>(out, points, pbase, idx, scalars, vsel, k, n, L);
     else
         k_small_msm<Fp2><<<blocks_for(L * k, WARP), WARP, 0, s>>>(out, points, pbase, idx, scalars, vsel, k, n, L);
+}
+
+void launch_decompress(Group g, uint8_t* out, uint8_t* status, const uint8_t* in, int64_t n, bool check_group,
+                       cudaStream_t s) {
+    ProfScope prof_("decompress", s);
+    if (n <= 0) return;
+    note_launch();
+    if (g == GROUP_G1) k_g1_decompress<<<blocks_for(n), TPB, 0, s>>>(out, status, in, n, check_group ? 1 : 0);
+    else k_g2_decompress<<<blocks_for(n), TPB, 0, s>>>(out, status, in, n, check_group ? 1 : 0);
 }
 
 void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {

@@ -71,6 +71,11 @@ void launch_group_ntt(Group g, uint8_t* io_affine, uint8_t* work_xyzz, const uin
                       int64_t count = 1);
 // compressed (ZCash) encodings
 void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
+// ZCash-format decoding with canonical-x, curve and (check_group) subgroup
+// checks; status[i] = 0 ok, 1 bad encoding, 2 not on the curve, 3 not in the
+// prime-order subgroup (the point is written as the identity then)
+void launch_decompress(Group g, uint8_t* out, uint8_t* status, const uint8_t* in, int64_t n, bool check_group,
+                       cudaStream_t s);
 // valid[i] = ([s_i] G == R_i + [c_i] X_i), G the G1 generator
 void launch_schnorr_verify(uint8_t* valid, const uint8_t* X, const uint8_t* R, const uint8_t* s_resp, const uint8_t* c, int64_t n, cudaStream_t st);
 

@@ -501,6 +501,41 @@ static int32_t compress_impl(wbte_ctx* ctx, Group g, void* out, const void* in, 
     if (c.ok()) launch_compress(g, d, s, (int64_t)n, c.s);
     return c.finish();
 }
+static int32_t decompress_impl(wbte_ctx* ctx, Group g, void* out, uint8_t* status, const void* in, uint64_t n,
+                               int32_t check_group) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !in) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    const size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    uint8_t* d = c.out(out, aff * n);
+    const uint8_t* s = c.in(in, (aff / 2) * n);
+    uint8_t* st = status ? c.out(status, n) : c.alloc(n);
+    if (!c.ok()) return c.finish();
+    launch_decompress(g, d, st, s, (int64_t)n, check_group != 0, c.s);
+    std::vector<uint8_t> h(n);
+    if (c.to_host(h.data(), st, n)) {
+        uint64_t bad = 0, first = n;
+        for (uint64_t i = 0; i < n; i++)
+            if (h[i]) {
+                bad++;
+                if (first == n) first = i;
+            }
+        if (bad) {
+            static const char* why[4] = {"", "bad encoding", "not on the curve", "not in the prime-order subgroup"};
+            c.fail(WBTE_ERR_NOT_ON_CURVE, std::to_string(bad) + " of " + std::to_string(n) +
+                                              " points rejected; first at " + std::to_string(first) + ": " +
+                                              why[h[first] < 4 ? h[first] : 1]);
+        }
+    }
+    return c.finish();
+}
+int32_t wbte_g1_decompress(wbte_ctx* ctx, void* out, uint8_t* status, const void* in, uint64_t n, int32_t check_group) {
+    return decompress_impl(ctx, GROUP_G1, out, status, in, n, check_group);
+}
+int32_t wbte_g2_decompress(wbte_ctx* ctx, void* out, uint8_t* status, const void* in, uint64_t n, int32_t check_group) {
+    return decompress_impl(ctx, GROUP_G2, out, status, in, n, check_group);
+}
 int32_t wbte_g1_compress(wbte_ctx* ctx, void* out, const void* in, uint64_t n) { return compress_impl(ctx, GROUP_G1, out, in, n); }
 int32_t wbte_g2_compress(wbte_ctx* ctx, void* out, const void* in, uint64_t n) { return compress_impl(ctx, GROUP_G2, out, in, n); }
 

@@ -129,6 +129,29 @@ def g2_compress(points, n: int | None = None):
 
 
 # -------------------------------------------------------- transforms
+def _decompress(name: str, size: int, blob, check_group: bool):
+    n = _nbytes(blob) // (size // 2)
+    out = bytearray(size * n)
+    status = np.zeros(max(1, n), dtype=np.uint8)
+    try:
+        ctx().call(name, out, status, blob, n, int(check_group))
+    except _lib.WbteError as err:
+        if err.status != -6:  # WBTE_ERR_NOT_ON_CURVE: the per-point status says which
+            raise
+    return bytes(out), [int(x) for x in status[:n]]
+
+
+def g1_decompress(blob, check_group: bool = True):
+    """Affine points and per-point status (0 ok, 1 bad encoding, 2 not on the
+    curve, 3 not in the subgroup) of 48-byte compressed G1 points."""
+    return _decompress("wbte_g1_decompress", G1_BYTES, blob, check_group)
+
+
+def g2_decompress(blob, check_group: bool = True):
+    """As g1_decompress for 96-byte compressed G2 points."""
+    return _decompress("wbte_g2_decompress", G2_BYTES, blob, check_group)
+
+
 def g1_ntt(points, inverse=False):
     buf = bytearray(points)
     ctx().call("wbte_g1_ntt", buf, len(buf) // G1_BYTES, int(inverse))
