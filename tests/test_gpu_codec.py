@@ -125,3 +125,33 @@ def test_key_material_round_trips_through_the_wire_format():
     out, status = ops.g2_decompress(blob)
     assert status == [0] * 4096 and out == pts
     assert wb.to_host(wb.to_device(pts)) == pts
+
+
+def test_public_decryption_key_wire_round_trip():
+    """weighted_btx key material written as compressed G2 streams and loaded
+    back through the checked device decoder decrypts the same batch; a
+    corrupted point is refused."""
+    from weighted_bte_b200 import weighted_btx as wb
+    from weighted_bte_b200.rng import ChaCha20Rng
+
+    rng = ChaCha20Rng.seed_from_u64(13)
+    mat = wb.keygen_with_rng(wb.KeygenConfig(4, [3, 2, 4], 4), rng)
+    dk = mat.decryption_key
+    blob = dk.to_wire()
+    assert len(blob) > 96 * (4 * 3 + 4 * 9 + 3 * 9)
+    dk2 = wb.PublicDecryptionKey.from_wire(blob)
+    assert dk2.setup_id() == dk.setup_id() and dk2.party_weights() == dk.party_weights()
+    assert dk2.domain_points() == dk.domain_points() and dk2.threshold_weight() == dk.threshold_weight()
+    for power in (1, 4):
+        assert dk2.verification_power(power) == dk.verification_power(power)
+        assert dk2.negative_power(power) == dk.negative_power(power)
+    assert dk2.positive_power(3) == dk.positive_power(3)
+    msgs = wb.messages_from_bytes([bytes([i]) * 32 for i in range(4)])
+    cts = wb.encrypt_many(mat.encryption_key, msgs, rng)
+    batch = wb.validate_batch(dk2, cts)
+    shares = wb.partial_decrypt_many([mat.party_keys[0], mat.party_keys[2]], batch)
+    assert wb.decrypt(dk2, cts, shares) == msgs
+    bad = bytearray(blob)
+    bad[-96 * 5 + 20] ^= 0x01  # a point of the positive material
+    with pytest.raises(ValueError):
+        wb.PublicDecryptionKey.from_wire(bytes(bad))

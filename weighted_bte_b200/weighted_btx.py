@@ -32,6 +32,7 @@ SETUP_ID_DOMAIN = b"WEIGHTED-BTX-SETUP-ID-v1"
 TRANSCRIPT_DOMAIN = b"WEIGHTED-BTX-SCHNORR-BLS12381-v1"
 BATCH_DIGEST_DOMAIN = b"WEIGHTED-BTX-ORDERED-BATCH-v1"
 DECRYPTION_CONTEXT_DOMAIN = b"WEIGHTED-BTX-DECRYPTION-CONTEXT-v1"
+WIRE_MAGIC = b"WBTE-WBTX-PUBLIC-DECRYPTION-KEY-v1"
 G1_IDENTITY = bytes(G1B)
 ROOT_OF_UNITY = pow(7, (R - 1) >> 32, R)
 TWO_ADICITY = 32
@@ -284,6 +285,58 @@ class PublicDecryptionKey:
         self._validate_power(power, max(0, self._max_batch_size - 1))
         W = self._total_weight
         return ops.split(to_host(self.positive_material[G2B * (power - 1) * W : G2B * power * W]), G2B)
+
+    # ------------------------------------------------------- wire format
+    def to_wire(self) -> bytes:
+        """The key as bytes: a header (WIRE_MAGIC, batch size, threshold, total
+        weight, domain size, party count, setup id, party weights), the
+        evaluation domain as 32-byte scalars, then the verification keys and
+        the negative and positive material as compressed G2 points (96 bytes
+        each, the crates' serialized size, weighted_pfe/README.md:159-214),
+        compressed on the device."""
+        B, N, W = self._max_batch_size, self.party_count(), self._total_weight
+        head = WIRE_MAGIC + struct.pack("<5Q", B, self._threshold_weight, W, self._domain_size, N)
+        head += self._setup_id + struct.pack(f"<{N}Q", *self._party_weights)
+        domain = b"".join(fr_bytes(x) for x in self._evaluation_domain)
+        streams = [ops.g2_compress(t, n) if n else b"" for t, n in
+                   ((self.verification_keys, B * N), (self.negative_material, B * W),
+                    (self.positive_material, (B - 1) * W))]
+        return head + domain + b"".join(streams)
+
+    @classmethod
+    def from_wire(cls, blob: bytes, check_group: bool = True, device: int = 0) -> "PublicDecryptionKey":
+        """Load a key written by to_wire: the compressed G2 streams are decoded
+        on the device straight into the resident arrays, each point checked
+        (canonical encoding, on the curve, and with check_group in the
+        prime-order subgroup), as blstrs' checked deserialization does."""
+        if not blob.startswith(WIRE_MAGIC):
+            raise ValueError("not a weighted_btx public decryption key")
+        o = len(WIRE_MAGIC)
+        B, t, W, domain_size, N = struct.unpack_from("<5Q", blob, o)
+        o += 40
+        setup_id = blob[o : o + 32]
+        o += 32
+        weights = list(struct.unpack_from(f"<{N}Q", blob, o))
+        o += 8 * N
+        if sum(weights) != W or B == 0:
+            raise ValueError("inconsistent key header")
+        domain = [int.from_bytes(blob[o + 32 * i : o + 32 * (i + 1)], "little") for i in range(W)]
+        o += 32 * W
+        counts = (B * N, B * W, (B - 1) * W)
+        if len(blob) != o + 96 * sum(counts):
+            raise ValueError("key material has the wrong length")
+        arrays = []
+        for n in counts:
+            out = empty_device(G2B * max(1, n), device)
+            if n:
+                try:
+                    _ctx().call("wbte_g2_decompress", out, None, blob[o : o + 96 * n], n, int(check_group))
+                except _lib.WbteError as err:
+                    raise ValueError(f"invalid key material: {err}") from None
+            arrays.append(out)
+            o += 96 * n
+        offsets = np.concatenate([[0], np.cumsum(weights)]).astype(np.int64)
+        return cls(setup_id, B, t, W, domain_size, weights, offsets, domain, *arrays)
 
     def abi_key(self) -> _lib.WbtxKey:
         k = _lib.WbtxKey()
