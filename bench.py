@@ -340,6 +340,7 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     torch.cuda.set_device(local)
     from weighted_bte_b200 import _lib
+    from weighted_bte_b200 import ops
     from weighted_bte_b200 import serving
     from weighted_bte_b200 import weighted_btx as wb
     from weighted_bte_b200.rng import ChaCha20Rng
@@ -365,6 +366,26 @@ def main():
     flush = torch.zeros(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup
+
+    # loading key material from its wire format: a slice of the CRS as
+    # compressed G2 points (96 B), decoded and checked on the device (canonical
+    # x, square root on the curve, [r]P = O), host bytes in, HBM out
+    n_crs = min(1 << 18, B * sum(weights))
+    crs_blob = ops.g2_compress(dk.negative_material, n_crs)
+    crs_out = torch.empty(192 * n_crs, dtype=torch.uint8, device="cuda")
+    crs_load = {}
+    for check in (True, False):
+        _lib.default_context(local).call("wbte_g2_decompress", crs_out, None, crs_blob[: 96 * 1024], 1024, int(check))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _lib.default_context(local).call("wbte_g2_decompress", crs_out, None, crs_blob, n_crs, int(check))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        crs_load["subgroup_checked" if check else "curve_checked_only"] = {
+            "points_per_s": round(n_crs / dt), "compressed_MB_per_s": round(96 * n_crs / dt / 1e6, 1)}
+    assert torch.equal(crs_out, dk.negative_material[: 192 * n_crs])
+    crs_load.update({"points": n_crs, "timing": "wall clock of the call, host-to-device copy included"})
+    del crs_out
 
     def step_plain(rb):
         return serving.decrypt_request(dk, rb, keys, ChaCha20Rng.seed_from_u64(99), None, device_output=True)
@@ -573,7 +594,7 @@ def main():
             "batched_over_plain": value / plain_value,
             "e2e": e2e, "gpu_launches": int(launches_b), "roofline": roofline, "roofline_plain": plain_roof,
             "cpu_baseline": cpu, "clocks": clocks, "kernel_ms_per_batch_plain": phases,
-            "kernel_ms_per_group": group_kernels, "setup_s": round(setup_s, 2),
+            "kernel_ms_per_group": group_kernels, "setup_s": round(setup_s, 2), "crs_load": crs_load,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
