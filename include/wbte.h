@@ -288,7 +288,16 @@ int32_t wbte_wbtx_partial_decrypt_many(wbte_ctx *ctx, void *sigma, const void *f
                                        const void *q, uint64_t T, uint64_t K);
 int32_t wbte_wbtx_verify_shares_many(wbte_ctx *ctx, int32_t *ok, const wbte_wbtx_key *key, const void *first,
                                      uint64_t batch_size, const void *sigma, const int64_t *party_indices,
-                                     const void *challenges, uint64_t T, uint64_t K);
+                                     const void *challenges, uint64_t T, uint64_t K, const void *vk_tables);
+/* Fixed-base tables of the verification keys of T parties at slots
+ * 1..batch_size (the points the share check aggregates with the challenges,
+ * weighted_btx/src/decryption.rs:358-422): T * batch_size tables of
+ * 11 * 32 affine G2 points ([m 64^w] vk, 67,584 bytes each), party-major.
+ * Given to verify_shares_many as vk_tables (NULL: Pippenger over the keys),
+ * each aggregate takes one mixed addition per nonzero signed radix-64 digit
+ * of the challenges' base-|x| digits and no doublings. */
+int32_t wbte_wbtx_vk_tables(wbte_ctx *ctx, void *tables, const wbte_wbtx_key *key, const int64_t *party_indices,
+                            uint64_t T, uint64_t batch_size);
 int32_t wbte_wbtx_precompute_many(wbte_ctx *ctx, void *beta, const void *kernel_lines, const void *first,
                                   const uint8_t *valid, uint64_t batch_size, uint64_t K);
 int32_t wbte_wbtx_open_many(wbte_ctx *ctx, void *messages, const void *opening_keys, const void *opening_lines,

@@ -2,6 +2,7 @@
 whether it runs alone (the plain `decrypt` path) or in a mix of concurrent
 requests of different batch sizes and committees, with and without the
 committee cache, and admission respects the HBM budget."""
+import numpy as np
 import pytest
 
 from weighted_bte_b200 import serving
@@ -122,3 +123,40 @@ def test_validate_batches_equals_validate_batch(mix):
         assert v.valid_mask() == one.valid_mask()
         assert wb.to_host(v.first_dev) == wb.to_host(one.first_dev)
         assert wb.to_host(v.valid_dev) == wb.to_host(one.valid_dev)
+
+
+def test_fixed_base_share_check_matches_pippenger():
+    """The share check over fixed-base tables of the parties' verification
+    keys accepts exactly what the Pippenger path accepts: honest shares of
+    every batch, not a batch with a tampered share."""
+    from weighted_bte_b200 import _lib
+    from weighted_bte_b200.rng import ChaCha20Rng, sample_nonzero
+
+    rng = ChaCha20Rng.seed_from_u64(21)
+    mat = wb.keygen_with_rng(wb.KeygenConfig(8, [3, 2, 4, 1], 4), rng)
+    dk = mat.decryption_key
+    keys = [mat.party_keys[0], mat.party_keys[2], mat.party_keys[3]]
+    K, B, T = 3, 8, len(keys)
+    batches = []
+    for _ in range(K):
+        msgs = wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(B)])
+        batches.append(wb.validate_batch(dk, wb.encrypt_many(mat.encryption_key, msgs, rng)))
+    import torch
+
+    first = torch.cat([v.first_dev[: 96 * B] for v in batches])
+    sig = b"".join(s.sigma for v in batches for s in wb.partial_decrypt_many(keys, v))
+    parties = [k.party_index for k in keys]
+    ch = b"".join(wb.fr_bytes(sample_nonzero(rng)) for _ in range(K * T))
+    tables = wb.empty_device(_lib.FIXED_TABLE_BYTES * T * B)
+    ctx = wb._ctx()
+    ctx.call("wbte_wbtx_vk_tables", tables, dk.abi_key(), _lib.i64_array(parties), T, B)
+    bad = bytearray(sig)
+    bad[96 * (1 * T + 2) + 7] ^= 0x04  # batch 1, third share
+    for s, expect in ((sig, [1, 1, 1]), (bytes(bad), [1, 0, 1])):
+        got = {}
+        for name, tab in (("tables", tables), ("pippenger", None)):
+            ok = np.zeros(K, dtype=np.int32)
+            ctx.call("wbte_wbtx_verify_shares_many", ok, dk.abi_key(), first, B, s, _lib.i64_array(parties), ch, T,
+                     K, tab)
+            got[name] = list(ok)
+        assert got["tables"] == got["pippenger"] == expect

@@ -33,6 +33,7 @@ STATUS_NAMES = {
 FE_FULL, FE_EASY, FE_HARD = 0, 1, 2
 CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 G1_BYTES, G2_BYTES, GT_BYTES, FR_BYTES, LINE_BYTES, MILLER_LINES = 96, 192, 576, 32, 288, 68
+FIXED_TABLE_BYTES = 192 * 11 * 32  # fixed-base table of one G2 point (wbte_wbtx_vk_tables)
 
 
 class LibraryMissing(RuntimeError):
@@ -141,7 +142,8 @@ _SIGNATURES = {
     "wbte_wpfe_precompute": [_VP, _VP, _VP, _VP, _U64],
     "wbte_wpfe_open": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64],
     "wbte_wbtx_partial_decrypt_many": [_VP, _VP, _U64, _VP, _U64, _U64],
-    "wbte_wbtx_verify_shares_many": [_VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64, _U64],
+    "wbte_wbtx_verify_shares_many": [_VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64, _U64, _VP],
+    "wbte_wbtx_vk_tables": [_VP, _VP, _VP, _U64, _U64],
     "wbte_wbtx_precompute_many": [_VP, _VP, _VP, _VP, _U64, _U64],
     "wbte_wbtx_open_many": [_VP, _VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64, _U64],
     "wbte_wbtx_decrypt_many": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64, _U64],

@@ -899,6 +899,77 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
     }
 }
 
+// ------------------------------------------- fixed-base G2 MSMs of few terms
+// For G2 points that stay fixed across many calls (a committee's verification
+// keys), table[p][w][m - 1] = [m 64^w] P_p (w < FB_WINDOWS, 1 <= m <= 32,
+// affine).  A term [s]P then costs one mixed addition per nonzero signed
+// radix-64 digit of each base-|x| digit of s (digit c acting through
+// (-1)^c psi^c, applied to the table entry), and no doublings.
+constexpr int FB_WINDOWS = 11, FB_ENTRIES = 32;  // 64-bit digits, radix 64
+
+// signed radix-64 digit k of d (d < 2^64): digits in [-31, 32], the carry
+// into digit k set when the low k digits of d exceed 0x20..20 (32 in each)
+WBTE_INL int r64_digit(uint64_t d, int k) {
+    auto carry = [&](int j) -> int {
+        if (j == 0 || 6 * j > 64) return 0;  // above bit 64 the bound exceeds any d < 2^64
+        const uint64_t m = (1ull << (6 * j)) - 1;
+        const uint64_t e = 0x820820820820820ull & m;  // 32 * 64^i summed over i < j
+        return (d & m) > e;
+    };
+    const int nib = 6 * k < 64 ? (int)((d >> (6 * k)) & 63u) : 0;
+    return nib + carry(k) - 64 * carry(k + 1);
+}
+
+__global__ void k_fixed_tables_g2(uint8_t* tables, const uint8_t* points, const int64_t* point_index, int64_t np) {
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= np * FB_WINDOWS) return;
+    const int64_t p = g / FB_WINDOWS;
+    const int w = (int)(g % FB_WINDOWS);
+    G2X base = from_affine(load_affine(reinterpret_cast<const G2A*>(points) + point_index[p]));
+    for (int i = 0; i < 6 * w; i++) base = xyzz_dbl(base);
+    G2A* T = reinterpret_cast<G2A*>(tables) + (p * FB_WINDOWS + w) * FB_ENTRIES;
+    G2X acc = base;
+    for (int m = 1; m <= FB_ENTRIES; m++) {
+        store_affine(T + m - 1, to_affine(acc));
+        if (m < FB_ENTRIES) acc = xyzz_add(acc, base);
+    }
+}
+
+// psi on an affine G2 point (the identity stays the identity)
+WBTE_INL G2A g2a_psi(const G2A& a) {
+    if (is_inf(a)) return a;
+    return G2A{fp2_mul(fp2_conj(a.x), fp2_from_const(C_PSI_CX)), fp2_mul(fp2_conj(a.y), fp2_from_const(C_PSI_CY))};
+}
+
+// out[o] = sum_t scalars[vsel[o] n + t] * P(tbase[o] + tidx[t]), one thread per output
+__global__ void __launch_bounds__(WARP) k_fixed_msm_g2(uint8_t* out, const uint8_t* tables, const int64_t* tbase,
+                                                      const int32_t* tidx, const uint8_t* scalars,
+                                                      const int32_t* vsel, int64_t k, int64_t n) {
+    const int64_t o = (int64_t)blockIdx.x * WARP + threadIdx.x;
+    if (o >= k) return;
+    const int64_t v = vsel ? (int64_t)vsel[o] : 0;
+    G2X acc;
+    set_inf(acc);
+    for (int64_t t = 0; t < n; t++) {
+        const G2A* T = reinterpret_cast<const G2A*>(tables) +
+                       (tbase[o] + (tidx ? (int64_t)tidx[t] : t)) * (FB_WINDOWS * FB_ENTRIES);
+        uint32_t sc[8];
+        load_scalar(sc, scalars + FR_SZ * (v * n + t));
+        uint64_t d[4];
+        decompose_base_x(d, sc);
+        for (int c = 0; c < 4; c++)
+            for (int w = 0; w < FB_WINDOWS; w++) {
+                const int dd = r64_digit(d[c], w);
+                if (!dd) continue;
+                G2A m = load_affine(T + w * FB_ENTRIES + (dd < 0 ? -dd : dd) - 1);
+                for (int i = 0; i < c; i++) m = g2a_psi(m);
+                if (((c & 1) != 0) != (dd < 0)) m.y = fp2_neg(m.y);
+                acc = xyzz_madd(acc, m);
+            }
+    }
+    store_affine(reinterpret_cast<G2A*>(out + G2_AFF * o), to_affine(acc));
+}
+
 // Lanes per small-MSM output, from a cost model: a lane's work is its
 // tables (7 additions per term it touches; 15 on G1, two tables), the shared
 // doublings and one addition per window and pair it holds; the launch takes
@@ -961,6 +1032,21 @@ void launch_decompress(Group g, uint8_t* out, uint8_t* status, const uint8_t* in
     note_launch();
     if (g == GROUP_G1) k_g1_decompress<<<blocks_for(n), TPB, 0, s>>>(out, status, in, n, check_group ? 1 : 0);
     else k_g2_decompress<<<blocks_for(n), TPB, 0, s>>>(out, status, in, n, check_group ? 1 : 0);
+}
+
+void launch_fixed_tables_g2(uint8_t* tables, const uint8_t* points, const int64_t* point_index, int64_t np,
+                            cudaStream_t s) {
+    ProfScope prof_("fixed_tables_g2", s);
+    if (np <= 0) return;
+    note_launch();
+    k_fixed_tables_g2<<<blocks_for(np * FB_WINDOWS), TPB, 0, s>>>(tables, points, point_index, np);
+}
+void launch_fixed_msm_g2(uint8_t* out, const uint8_t* tables, const int64_t* tbase, const int32_t* tidx,
+                         const uint8_t* scalars, const int32_t* vsel, int64_t k, int64_t n, cudaStream_t s) {
+    ProfScope prof_("fixed_msm_g2", s);
+    if (k <= 0) return;
+    note_launch();
+    k_fixed_msm_g2<<<blocks_for(k, WARP), WARP, 0, s>>>(out, tables, tbase, tidx, scalars, vsel, k, n);
 }
 
 void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {

@@ -71,6 +71,13 @@ void launch_group_ntt(Group g, uint8_t* io_affine, uint8_t* work_xyzz, const uin
                       int64_t count = 1);
 // compressed (ZCash) encodings
 void launch_compress(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
+// fixed-base tables of np G2 points (points[point_index[p]]): FIXED_TABLE_BYTES each
+constexpr size_t FIXED_TABLE_BYTES = G2_AFF * 11 * 32;
+void launch_fixed_tables_g2(uint8_t* tables, const uint8_t* points, const int64_t* point_index, int64_t np,
+                            cudaStream_t s);
+// out[o] = sum_t scalars[vsel[o] n + t] * (point of table tbase[o] + tidx[t]), k outputs
+void launch_fixed_msm_g2(uint8_t* out, const uint8_t* tables, const int64_t* tbase, const int32_t* tidx,
+                         const uint8_t* scalars, const int32_t* vsel, int64_t k, int64_t n, cudaStream_t s);
 // ZCash-format decoding with canonical-x, curve and (check_group) subgroup
 // checks; status[i] = 0 ok, 1 bad encoding, 2 not on the curve, 3 not in the
 // prime-order subgroup (the point is written as the identity then)

@@ -1708,9 +1708,30 @@ int32_t wbte_wbtx_partial_decrypt_many(wbte_ctx* ctx, void* sigma, const void* f
     return c.finish();
 }
 
+int32_t wbte_wbtx_vk_tables(wbte_ctx* ctx, void* tables, const wbte_wbtx_key* key, const int64_t* party_indices,
+                            uint64_t T, uint64_t B) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (check_key(c, key)) return c.finish();
+    if (T == 0 || B == 0) return c.finish();
+    if (!tables || !party_indices) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    if (B > key->max_batch_size) return c.fail(WBTE_ERR_SIZE, "batch size out of range");
+    const uint64_t N = key->party_count;
+    std::vector<int64_t> idx(T * B);
+    for (uint64_t t = 0; t < T; t++) {
+        if (party_indices[t] < 0 || (uint64_t)party_indices[t] >= N) return c.fail(WBTE_ERR_INVALID_ARG, "invalid party index");
+        for (uint64_t i = 0; i < B; i++) idx[t * B + i] = (int64_t)(i * N) + party_indices[t];
+    }
+    uint8_t* d = c.out(tables, FIXED_TABLE_BYTES * T * B);
+    const uint8_t* dvk = c.in(key->verification_keys, G2_AFF * key->max_batch_size * N);
+    const int64_t* didx = c.in_vec(idx);
+    if (c.ok()) launch_fixed_tables_g2(d, dvk, didx, (int64_t)(T * B), c.s);
+    return c.finish();
+}
+
 int32_t wbte_wbtx_verify_shares_many(wbte_ctx* ctx, int32_t* ok, const wbte_wbtx_key* key, const void* first, uint64_t B,
                                      const void* sigma, const int64_t* party_indices, const void* challenges,
-                                     uint64_t T, uint64_t K) {
+                                     uint64_t T, uint64_t K, const void* vk_tables) {
     if (!ctx) return WBTE_ERR_INVALID_ARG;
     Call c(ctx);
     if (!ok) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
@@ -1762,7 +1783,21 @@ int32_t wbte_wbtx_verify_shares_many(wbte_ctx* ctx, int32_t* ok, const wbte_wbtx
     if (!c.ok()) return c.finish();
     launch_msm_family(GROUP_G1, agg, dsig, dsbase, nullptr, dch, dsvsel, (int32_t)K, (int64_t)K, (int64_t)T, c.s);
     launch_negate(GROUP_G1, agg, agg, (int64_t)K, c.s);
-    launch_msm_family(GROUP_G2, aggvk, dvk, dvbase, dpidx, dch, dvvsel, (int32_t)K, (int64_t)(B * K), (int64_t)T, c.s);
+    if (vk_tables) {
+        // the committee's fixed-base tables: table t B + i holds party t's key at slot i
+        std::vector<int64_t> tbase(B * K);
+        std::vector<int32_t> tidx(T);
+        for (uint64_t b = 0; b < K; b++)
+            for (uint64_t i = 0; i < B; i++) tbase[b * B + i] = (int64_t)i;
+        for (uint64_t t = 0; t < T; t++) tidx[t] = (int32_t)(t * B);
+        const uint8_t* dtab = c.in(vk_tables, FIXED_TABLE_BYTES * T * B);
+        const int64_t* dtbase = c.in_vec(tbase);
+        const int32_t* dtidx = c.in_vec(tidx);
+        if (!c.ok()) return c.finish();
+        launch_fixed_msm_g2(aggvk, dtab, dtbase, dtidx, dch, dvvsel, (int64_t)(B * K), (int64_t)T, c.s);
+    } else {
+        launch_msm_family(GROUP_G2, aggvk, dvk, dvbase, dpidx, dch, dvvsel, (int32_t)K, (int64_t)(B * K), (int64_t)T, c.s);
+    }
     cudaMemcpy2DAsync(P, G1_AFF * P1, dfirst, G1_AFF * B, G1_AFF * B, K, cudaMemcpyDeviceToDevice, c.s);
     cudaMemcpy2DAsync(P + G1_AFF * B, G1_AFF * P1, agg, G1_AFF, G1_AFF, K, cudaMemcpyDeviceToDevice, c.s);
     cudaMemcpy2DAsync(Q, G2_AFF * P1, aggvk, G2_AFF * B, G2_AFF * B, K, cudaMemcpyDeviceToDevice, c.s);

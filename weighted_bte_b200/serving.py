@@ -37,6 +37,7 @@ mix.
 from __future__ import annotations
 
 import collections
+import struct
 import concurrent.futures as cf
 import threading
 import time
@@ -140,6 +141,48 @@ class CommitteeCache:
             t.record_stream(stream)
         return entry.pre
 
+    def vk_tables(self, dk: wb.PublicDecryptionKey, batch_size: int, party_indices: Sequence[int]):
+        """Fixed-base tables of the parties' verification keys at slots
+        1..batch_size (wbte_wbtx_vk_tables), built once per party set and
+        batch size on the calling thread's current stream; the share check of
+        every later group of the same parties uses them."""
+        torch = wb._t()
+        key = b"vk-tables" + dk.setup_id() + struct.pack("<Q", batch_size) + b"".join(
+            struct.pack("<q", j) for j in party_indices)
+        with self._lock:
+            entry = self._entries.get(key)
+            owner = entry is None
+            if owner:
+                entry = _Entry()
+                self._entries[key] = entry
+            else:
+                self._entries.move_to_end(key)
+        if owner:
+            try:
+                T = len(party_indices)
+                tables = wb.empty_device(_lib.FIXED_TABLE_BYTES * T * batch_size)
+                wb._ctx().call("wbte_wbtx_vk_tables", tables, dk.abi_key(), _lib.i64_array(party_indices), T,
+                               batch_size)
+                ev = torch.cuda.Event()
+                ev.record(torch.cuda.current_stream())
+                entry.pre, entry.ready, entry.nbytes = tables, ev, tables.numel()
+            except BaseException as exc:  # noqa: BLE001 -- handed to every waiter
+                entry.error = exc
+                with self._lock:
+                    self._entries.pop(key, None)
+            finally:
+                entry.done.set()
+            if entry.error is None:
+                self._evict()
+        else:
+            entry.done.wait()
+        if entry.error is not None:
+            raise entry.error
+        stream = torch.cuda.current_stream()
+        stream.wait_event(entry.ready)
+        entry.pre.record_stream(stream)
+        return entry.pre
+
     def _evict(self):
         with self._lock:
             self._bytes = sum(e.nbytes for e in self._entries.values())
@@ -206,9 +249,10 @@ def decrypt_group(dk: wb.PublicDecryptionKey, batches: Sequence, party_keys: Seq
 
         challenges = [[sample_nonzero(rng) for _ in range(T)] for _ in range(K)]
         ok = np.zeros(K, dtype=np.int32)
-        ctx.call("wbte_wbtx_verify_shares_many", ok, dk.abi_key(), first, B, bytes(sig),
-                 _lib.i64_array([pk.party_index for pk in party_keys]),
-                 b"".join(wb.fr_bytes(c) for row in challenges for c in row), T, K)
+        parties = [pk.party_index for pk in party_keys]
+        tables = cache.vk_tables(dk, B, parties) if cache is not None else None
+        ctx.call("wbte_wbtx_verify_shares_many", ok, dk.abi_key(), first, B, bytes(sig), _lib.i64_array(parties),
+                 b"".join(wb.fr_bytes(c) for row in challenges for c in row), T, K, tables)
         accepted = [wb.finish_acceptance(dk, validated[b], *screened[b], bool(ok[b])) for b in range(K)]
     else:
         accepted = [wb.accept_decryption_shares(dk, validated[b], shares[b], rng) for b in range(K)]
