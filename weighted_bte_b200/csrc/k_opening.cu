@@ -1,0 +1,42 @@
+// The opening's multi-Miller loops over prepared line tables: one loop per
+// slot shares the Fp12 squarings across the slot's T pairings.  Built with
+// the library's default layout (out-of-line Fp2 products, inline Fp sums),
+// which runs this kernel faster than the inline-Fp2 layout of k_pairing.cu.
+#include "launch.h"
+#include "pairing.cuh"
+
+namespace wbte {
+
+namespace {
+constexpr int TPB = 64;
+inline unsigned blocks_for(int64_t n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+WBTE_INL Fp12* as_gt(uint8_t* p) { return reinterpret_cast<Fp12*>(p); }
+
+// out[o] = prod_{t < T} Miller(P[(o / per) * T + t], lines of table (o % per) * T + t):
+// the opening of K batches against one committee's prepared opening keys
+// (tables line-major with stride per * T), each batch with its own T shares.
+__global__ void k_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per,
+                                     int T) {
+    int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const int64_t b = o / per, i = o % per;
+    Fp12 f;
+    multi_miller_loop_lines(f, reinterpret_cast<const Line*>(lines) + i * T, (size_t)(per * T), 1,
+                            reinterpret_cast<const G1A*>(p) + b * T, T);
+    store_vec(as_gt(out) + o, f);
+}
+
+}  // namespace
+
+bool launch_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per, int T,
+                               cudaStream_t s) {
+    ProfScope prof_("miller_lines_multi", s);
+    if (T < 1 || T > MULTI_MILLER_MAX) return false;
+    if (n <= 0) return true;
+    note_launch();
+    k_miller_lines_multi<<<blocks_for(n), TPB, 0, s>>>(out, lines, p, n, per, T);
+    return true;
+}
+
+}  // namespace wbte

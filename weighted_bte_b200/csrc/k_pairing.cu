@@ -56,20 +56,6 @@ __global__ void WBTE_PAIR_BOUNDS k_miller_lines(uint8_t* out, const uint8_t* lin
     store_vec(as_gt(out) + i, f);
 }
 
-// out[o] = prod_{t < T} Miller(P[(o / per) * T + t], lines of table (o % per) * T + t):
-// the opening of K batches against one committee's prepared opening keys
-// (tables line-major with stride per * T), each batch with its own T shares.
-__global__ void WBTE_PAIR_BOUNDS k_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per,
-                                     int T) {
-    int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (o >= n) return;
-    const int64_t b = o / per, i = o % per;
-    Fp12 f;
-    multi_miller_loop_lines(f, reinterpret_cast<const Line*>(lines) + i * T, (size_t)(per * T), 1,
-                            reinterpret_cast<const G1A*>(p) + b * T, T);
-    store_vec(as_gt(out) + o, f);
-}
-
 __global__ void WBTE_PAIR_BOUNDS k_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, int64_t p_mod, int64_t q_mod) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -200,15 +186,6 @@ void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, 
     if (n <= 0) return;
     note_launch();
     k_miller<<<blocks_for(n), TPB, 0, s>>>(out, p, q, n, p_mod, q_mod);
-}
-bool launch_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per, int T,
-                               cudaStream_t s) {
-    ProfScope prof_("miller_lines_multi", s);
-    if (T < 1 || T > MULTI_MILLER_MAX) return false;
-    if (n <= 0) return true;
-    note_launch();
-    k_miller_lines_multi<<<blocks_for(n), TPB, 0, s>>>(out, lines, p, n, per, T);
-    return true;
 }
 void launch_fp12_mask(uint8_t* io, const uint8_t* valid, int64_t n, cudaStream_t s) {
     if (n <= 0) return;
