@@ -331,13 +331,11 @@ def main():
 
     import numpy as np
     import torch
-    import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    from weighted_bte_b200 import replicas
+
+    ranks = replicas.init("nccl")
+    world, rank, local = ranks.world, ranks.rank, ranks.local_rank
     torch.cuda.set_device(local)
     from weighted_bte_b200 import _lib
     from weighted_bte_b200 import ops
@@ -350,7 +348,7 @@ def main():
     weights, t = cfg.weights, cfg.threshold
     committee, _ = minimal_authorized_parties(weights, t)
     W_T = sum(weights[j] for j in committee)
-    rng = ChaCha20Rng.seed_from_u64(cfg.seed + 7919 * rank)
+    rng = ChaCha20Rng.seed_from_u64(ranks.seed(cfg.seed))
 
     t_setup = time.perf_counter()
     mat = wb.keygen_with_rng(wb.KeygenConfig(B, weights, t), rng)
@@ -392,16 +390,7 @@ def main():
 
     cache = serving.CommitteeCache(8 << 30)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world > 1:
-            t_all = torch.tensor([x], device="cuda")
-            dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
-            return float(t_all.item())
-        return x
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     # ---- plain: one batch per step on one stream, committee prepared every batch
     stream = torch.cuda.current_stream()
@@ -597,9 +586,7 @@ def main():
             "kernel_ms_per_group": group_kernels, "setup_s": round(setup_s, 2), "crs_load": crs_load,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":
