@@ -129,7 +129,7 @@ def parse_args():
                     help="batch size of the bounded CPU-oracle sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--concurrency", type=int, default=2, help="concurrent groups (streams) of the batched form")
+    ap.add_argument("--concurrency", type=int, default=3, help="concurrent groups (streams) of the batched form")
     ap.add_argument("--group", type=int, default=128, help="batches per group (one launch sequence) in the batched form")
     return ap.parse_args()
 
