@@ -35,6 +35,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import random
 import statistics
 import subprocess
 import sys
@@ -475,6 +476,33 @@ def main():
                "committee_cache": {"hits": st["cache_hits"], "misses": st["cache_misses"]},
                "timing": "wall clock from the first submit to the last host result; latency per request from "
                          "submit to host result; all requests submitted at once"}
+        # request latency under load: Poisson arrivals at half the served rate
+        # just measured, about 8 s of them, through a fresh server whose
+        # committee is prepared before the first arrival
+        req_rate = 0.5 * n_req / e2e_s
+        n_load = max(2 * C, min(4 * n_req, int(8 * req_rate)))
+        arrivals = random.Random(4 + rank)
+        with serving.DecryptionServer(dk, slots=C, max_group=G) as srv:
+            srv.submit(host_b[0], keys, seed=99).result()
+            srv.latencies.clear()
+            barrier()
+            t0 = time.perf_counter()
+            t_next, futs = t0, []
+            for i in range(n_load):
+                t_next += arrivals.expovariate(req_rate)
+                delay = t_next - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                futs.append(srv.submit(host_b[i % n_unique], keys, seed=99))
+            res = [f.result() for f in futs]
+            load_s = time.perf_counter() - t0
+            st = srv.stats()
+        for i, r in enumerate(res):
+            assert r == plain_b[i % n_unique], "served decryption mismatch"
+        e2e["at_load"] = {"offered_requests_per_s": round(req_rate, 1), "requests": n_load,
+                          "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                          "ciphertexts_per_s": round(B * n_load / load_s),
+                          "arrivals": "Poisson at half the served throughput above, per replica"}
 
     # ---- roofline.  Peak: the integer-pipe rate measured by a calibration
     # kernel, in Fp products per second.  The headline is the batched form's
