@@ -6,6 +6,8 @@ be CUDA tensors (resident in HBM); outputs are returned as `bytes` unless an
 """
 from __future__ import annotations
 
+from typing import Optional
+
 import numpy as np
 
 from . import _lib
@@ -14,8 +16,21 @@ from ._lib import FR_BYTES, G1_BYTES, G2_BYTES, GT_BYTES, LINE_BYTES, MILLER_LIN
 R = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001
 
 
-def ctx(device: int = 0) -> _lib.Context:
-    return _lib.default_context(device)
+def current_device() -> int:
+    """The calling thread's current CUDA device as torch sees it (0 before
+    torch is imported)."""
+    import sys
+
+    torch = sys.modules.get("torch")
+    if torch is not None and torch.cuda.is_available():
+        return torch.cuda.current_device()
+    return 0
+
+
+def ctx(device: Optional[int] = None) -> _lib.Context:
+    """The calling thread's library context on `device`, by default the
+    thread's current CUDA device."""
+    return _lib.default_context(current_device() if device is None else device)
 
 
 def scalars_bytes(scalars) -> bytes:

@@ -296,15 +296,15 @@ class DecryptionServer:
 
     def __init__(self, decryption_key: wb.PublicDecryptionKey, slots: int = 4,
                  hbm_budget_bytes: Optional[int] = None, cache_bytes: Optional[int] = None,
-                 device: int = 0, cache_committees: bool = True, max_group: int = 1):
+                 device: Optional[int] = None, cache_committees: bool = True, max_group: int = 1):
         torch = wb._t()
         self.dk = decryption_key
-        self.device = device
+        self.device = torch.cuda.current_device() if device is None else device
         # requests of one batch size and committee that wait together are
         # decrypted as one group (the batched form), up to max_group at a time
         self.max_group = max(1, int(max_group))
         if hbm_budget_bytes is None:
-            free, _total = torch.cuda.mem_get_info(device)
+            free, _total = torch.cuda.mem_get_info(self.device)
             hbm_budget_bytes = free // 2
         self.budget = int(hbm_budget_bytes)
         self.cache = CommitteeCache(cache_bytes if cache_bytes is not None else self.budget // 4) \

@@ -50,18 +50,21 @@ def _t():
     return _torch
 
 
-def _device(device: int = 0):
-    return _t().device("cuda", device)
+def _device(device: Optional[int] = None):
+    """The CUDA device `device`, by default the calling thread's current one
+    (each rank of a multi-GPU run works on its own)."""
+    torch = _t()
+    return torch.device("cuda", torch.cuda.current_device() if device is None else device)
 
 
-def to_device(data: bytes, device: int = 0):
+def to_device(data: bytes, device: Optional[int] = None):
     torch = _t()
     if len(data) == 0:
         return torch.empty(16, dtype=torch.uint8, device=_device(device))
     return torch.frombuffer(bytearray(data), dtype=torch.uint8).to(_device(device))
 
 
-def empty_device(nbytes: int, device: int = 0):
+def empty_device(nbytes: int, device: Optional[int] = None):
     return _t().empty(max(16, nbytes), dtype=torch_uint8(), device=_device(device))
 
 
@@ -304,7 +307,7 @@ class PublicDecryptionKey:
         return head + domain + b"".join(streams)
 
     @classmethod
-    def from_wire(cls, blob: bytes, check_group: bool = True, device: int = 0) -> "PublicDecryptionKey":
+    def from_wire(cls, blob: bytes, check_group: bool = True, device: Optional[int] = None) -> "PublicDecryptionKey":
         """Load a key written by to_wire: the compressed G2 streams are decoded
         on the device straight into the resident arrays, each point checked
         (canonical encoding, on the curve, and with check_group in the
