@@ -13,15 +13,20 @@ Two forms of the same work are timed, both bit-exact against the plaintexts:
   plain  : one batch per step on one stream, the committee prepared for every
            batch -- the reference's `decrypt()` sequence, one batch at a time
   value  : the batched form: each step runs C groups concurrently on C CUDA
-           streams, a group being G batches whose every GPU phase is one
-           launch over all of them; the committee preparation, which the reference
-           documents as reusable for the same batch size and party set
-           (weighted_btx/src/decryption.rs:424-426), is cached: the timed
-           region starts with an empty cache, so the first batch prepares
+           streams (default 3), a group being G batches (default 128) whose
+           every GPU phase is one launch over all of them; the committee
+           preparation, which the reference documents as reusable for the
+           same batch size and party set (weighted_btx/src/decryption.rs:424-426),
+           is cached with the parties' verification-key tables: the timed
+           region starts with an empty cache, so the first group prepares
   e2e    : the served form through the public API (serving.DecryptionServer)
            with host ciphertext objects and host results, wall clock, with
-           p50/p99 request latency
+           p50/p99 request latency (all requests submitted at once) and
+           `at_load`: p50/p99 under Poisson arrivals at half that rate
 
+Also reported: `roofline` (the dominant kernel of the batched form against the
+measured integer-pipe peak), `cpu_baseline` (the CPU restatement on the host
+cores), `crs_load` (checked decoding of compressed key material), `clocks`.
 Device times use CUDA events; L2 is flushed (256 MB write) before every
 step.
 
@@ -29,6 +34,7 @@ Multi-GPU: replicas only -- every rank decrypts its own batches with its own
 copy of the public key; no collective on the data path (scaling "weak").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
+                  [--concurrency C] [--group G] [--no-e2e] [--no-cpu-baseline]
 """
 from __future__ import annotations
 
