@@ -160,3 +160,51 @@ def test_fixed_base_share_check_matches_pippenger():
                      K, tab)
             got[name] = list(ok)
         assert got["tables"] == got["pippenger"] == expect
+
+
+def test_fused_decryption_matches_precompute_then_open():
+    """wbte_wbtx_decrypt_many (one hard final exponentiation per slot), with
+    and without the opening keys' line tables, equals precompute_many
+    followed by open_many, invalid slots included."""
+    from weighted_bte_b200 import _lib
+
+    rng = ChaCha20Rng.seed_from_u64(23)
+    mat = wb.keygen_with_rng(wb.KeygenConfig(8, [3, 2, 4, 1], 4), rng)
+    dk = mat.decryption_key
+    keys = [mat.party_keys[0], mat.party_keys[2]]
+    K, B, T = 2, 8, len(keys)
+    vals, cts_all = [], []
+    for b in range(K):
+        msgs = wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(B)])
+        cts = wb.encrypt_many(mat.encryption_key, msgs, rng)
+        if b == 1:  # an invalid proof at slot 3
+            cts[3] = wb.Ciphertext(cts[3].first, cts[3].second,
+                                   wb.SchnorrProof(cts[3].proof.commitment, (cts[3].proof.response + 1) % wb.R))
+        cts_all.append(cts)
+        vals.append(wb.validate_batch(dk, cts))
+    import torch
+
+    first = torch.cat([v.first_dev[: 96 * B] for v in vals])
+    valid = torch.cat([v.valid_dev[:B] for v in vals])
+    second = wb.to_device(b"".join(c.second for cts in cts_all for c in cts))
+    accepted = wb.accept_decryption_shares(dk, vals[0], wb.partial_decrypt_many(keys, vals[0]))
+    pre = wb.prepare_decryption(dk, accepted)
+    sig = b"".join(s.sigma for v in vals for s in wb.partial_decrypt_many(keys, v))
+    ctx = wb._ctx()
+    beta = wb.empty_device(576 * B * K)
+    ref = wb.empty_device(576 * B * K)
+    ctx.call("wbte_wbtx_precompute_many", beta, pre.kernel_lines, first, valid, B, K)
+    ctx.call("wbte_wbtx_open_many", ref, pre.opening_keys, pre.opening_lines, sig, T, second, beta, valid, B, K)
+    for lines in (pre.opening_lines, None):
+        out = wb.empty_device(576 * B * K)
+        ctx.call("wbte_wbtx_decrypt_many", out, pre.kernel_lines, pre.opening_keys, lines, first, second, valid,
+                 sig, T, B, K)
+        assert torch.equal(out[: 576 * B * K], ref[: 576 * B * K]), lines is None
+    host = wb.to_host(ref, 576 * B * K)
+    plain = [wb.decrypt(dk, cts, wb.partial_decrypt_many(keys, wb.validate_batch(dk, cts))) for cts in cts_all]
+    for b in range(K):
+        for i in range(B):
+            got = host[576 * (b * B + i) : 576 * (b * B + i + 1)]
+            assert (plain[b][i] is None) == (not vals[b].valid[i])
+            if plain[b][i] is not None:
+                assert got == plain[b][i]
