@@ -208,3 +208,20 @@ def test_fused_decryption_matches_precompute_then_open():
             assert (plain[b][i] is None) == (not vals[b].valid[i])
             if plain[b][i] is not None:
                 assert got == plain[b][i]
+
+
+def test_group_of_32_batches_matches_one_by_one():
+    """32 batches in one group: every batched transform runs its warp-uniform
+    kernels (the G1 transform's NAF twiddles, the GT stages' NAF plans)."""
+    rng = ChaCha20Rng.seed_from_u64(29)
+    mat = wb.keygen_with_rng(wb.KeygenConfig(8, [3, 2, 4, 1], 4), rng)
+    dk = mat.decryption_key
+    keys = [mat.party_keys[0], mat.party_keys[2]]
+    msgs, batches = [], []
+    for _ in range(32):
+        m = wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(8)])
+        msgs.append(m)
+        batches.append(wb.encrypt_many(mat.encryption_key, m, rng))
+    out = serving.decrypt_group(dk, [wb.CiphertextBatch.upload(c) for c in batches], keys,
+                                ChaCha20Rng.seed_from_u64(3), serving.CommitteeCache(1 << 30))
+    assert out == msgs

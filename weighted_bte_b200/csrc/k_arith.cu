@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <mutex>
+#include <type_traits>
 
 #include "launch.h"
 #include "pairing.cuh"
@@ -362,6 +363,68 @@ static __device__ __noinline__ Xyzz<F> mul_joint(const Xyzz<F> v, const uint8_t*
     return acc;
 }
 
+// width-5 NAF of the 128-bit w = hi 2^64 + lo: digits in {0, +-1, +-3, .., +-15},
+// least significant first; returns the length (at most 129)
+WBTE_INL int wnaf5_128(int8_t* dig, uint64_t lo, uint64_t hi) {
+    int len = 0;
+    while (lo | hi) {
+        int d = 0;
+        if (lo & 1) {
+            d = (int)(lo & 31);
+            if (d >= 16) d -= 32;
+            if (d > 0) {
+                const uint64_t n = lo - (uint64_t)d;
+                hi -= n > lo ? 1 : 0;
+                lo = n;
+            } else {
+                const uint64_t n = lo + (uint64_t)(-d);
+                hi += n < lo ? 1 : 0;
+                lo = n;
+            }
+        }
+        dig[len++] = (int8_t)d;
+        lo = (lo >> 1) | (hi << 63);
+        hi >>= 1;
+    }
+    return len;
+}
+
+// [k]v on G1 for a canonical scalar k by one thread: the two GLV digit groups
+// w_0, w_1 (v and phi(v) + v) in width-5 NAF over one run of doublings,
+// tables of odd multiples.  Control flow follows the digits, so it is meant
+// for warps whose threads share the scalar (no divergence then).
+static __device__ __noinline__ G1X g1_mul_joint_naf(const G1X v, const uint8_t* scalar) {
+    G1X tab[2][8];  // odd multiples 1, 3, .., 15 of v and of phi(v) + v
+    tab[0][0] = v;
+    tab[1][0] = xyzz_add(g1_phi(v), v);
+    for (int c = 0; c < 2; c++) {
+        const G1X two = xyzz_dbl(tab[c][0]);
+        for (int m = 1; m < 8; m++) tab[c][m] = xyzz_add(tab[c][m - 1], two);
+    }
+    uint32_t sc[8];
+    load_scalar(sc, scalar);
+    uint64_t d[4], lo[4], hi[4];
+    decompose_base_x(d, sc);
+    small_msm_digits(lo, hi, d, (const G1X*)nullptr);
+    int8_t naf[2][130];
+    const int l0 = wnaf5_128(naf[0], lo[0], hi[0]), l1 = wnaf5_128(naf[1], lo[1], hi[1]);
+    G1X acc;
+    set_inf(acc);
+    bool started = false;
+    for (int pos = (l0 > l1 ? l0 : l1) - 1; pos >= 0; pos--) {
+        if (started) acc = xyzz_dbl(acc);
+        for (int c = 0; c < 2; c++) {
+            const int dd = pos < (c ? l1 : l0) ? naf[c][pos] : 0;
+            if (!dd) continue;
+            G1X m = tab[c][((dd < 0 ? -dd : dd) - 1) >> 1];
+            if (dd < 0) m = neg(m);
+            acc = started ? xyzz_add(acc, m) : m;
+            started = true;
+        }
+    }
+    return acc;
+}
+
 // One radix-2 butterfly per thread with the twiddle multiplication on one
 // thread (mul_joint: the digit groups share their doublings), for batches of
 // transforms large enough to fill the GPU without the lane split.  Threads
@@ -376,7 +439,15 @@ __global__ void __launch_bounds__(WARP) k_ntt_stage_joint(uint8_t* work, const u
     const int64_t a = q * n + chunk * 2 * half + j, b = a + half;
     Xyzz<F>* w = reinterpret_cast<Xyzz<F>*>(work);
     Xyzz<F> t = load_vec(w + b);
-    if (j != 0) t = mul_joint(t, tw + FR_SZ * (j * (n / (2 * half))));
+    if (j != 0) {
+        const uint8_t* sc = tw + FR_SZ * (j * (n / (2 * half)));
+        if constexpr (std::is_same<F, Fp>::value) {
+            // whole warps share the twiddle when the transforms come in multiples of 32
+            t = count % WARP == 0 ? g1_mul_joint_naf(t, sc) : mul_joint(t, sc);
+        } else {
+            t = mul_joint(t, sc);
+        }
+    }
     const Xyzz<F> u = load_vec(w + a);
     store_vec(w + a, xyzz_add(u, t));
     store_vec(w + b, xyzz_add(u, neg(t)));
