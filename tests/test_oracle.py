@@ -219,3 +219,20 @@ def test_work_counts_reproduce(orc):
     plain = orc.lib()
     plain.orc_fp_product_count.restype = ctypes.c_ulonglong
     assert plain.orc_fp_product_count() == 0
+
+
+def test_vectorised_chacha20_blocks_equal_the_block_function():
+    import random
+
+    from weighted_bte_b200.rng import ChaCha20Rng, chacha20_block, chacha20_blocks
+
+    rng = random.Random(5)
+    key = [rng.getrandbits(32) for _ in range(8)]
+    for counter in (0, 1, (1 << 32) - 3, (1 << 40) + 7):
+        flat = chacha20_blocks(key, counter, 5)
+        for b in range(5):
+            assert flat[16 * b : 16 * (b + 1)] == chacha20_block(key, counter + b)
+    # the generator's stream does not depend on how many blocks a refill makes
+    a, b = ChaCha20Rng.seed_from_u64(9), ChaCha20Rng.seed_from_u64(9)
+    b.REFILL_BLOCKS = 1
+    assert [a.next_u64() for _ in range(300)] == [b.next_u64() for _ in range(300)]

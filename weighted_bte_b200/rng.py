@@ -56,6 +56,48 @@ def chacha20_block(key_words, counter: int, stream: int = 0):
     return [(w[i] + state[i]) & _M32 for i in range(16)]
 
 
+def chacha20_blocks(key_words, counter: int, n: int):
+    """n consecutive keystream blocks (counters counter .. counter + n - 1,
+    stream 0) as one flat list of 16 n words, computed for all blocks at once
+    with numpy uint32 vectors (the same function as chacha20_block)."""
+    import numpy as np
+
+    st = np.empty((16, n), dtype=np.uint32)
+    st[0:4] = np.array([0x61707865, 0x3320646E, 0x79622D32, 0x6B206574], dtype=np.uint32)[:, None]
+    st[4:12] = np.array(list(key_words), dtype=np.uint32)[:, None]
+    ctr = np.arange(counter, counter + n, dtype=np.uint64)
+    st[12] = (ctr & np.uint64(_M32)).astype(np.uint32)
+    st[13] = (ctr >> np.uint64(32)).astype(np.uint32)
+    st[14] = 0
+    st[15] = 0
+    w = [st[i].copy() for i in range(16)]
+
+    def rotl(x, k):
+        return (x << np.uint32(k)) | (x >> np.uint32(32 - k))
+
+    def quarter(a, b, c, d):
+        w[a] += w[b]
+        w[d] = rotl(w[d] ^ w[a], 16)
+        w[c] += w[d]
+        w[b] = rotl(w[b] ^ w[c], 12)
+        w[a] += w[b]
+        w[d] = rotl(w[d] ^ w[a], 8)
+        w[c] += w[d]
+        w[b] = rotl(w[b] ^ w[c], 7)
+
+    for _ in range(10):
+        quarter(0, 4, 8, 12)
+        quarter(1, 5, 9, 13)
+        quarter(2, 6, 10, 14)
+        quarter(3, 7, 11, 15)
+        quarter(0, 5, 10, 15)
+        quarter(1, 6, 11, 12)
+        quarter(2, 7, 8, 13)
+        quarter(3, 4, 9, 14)
+    out = np.stack(w) + st
+    return out.T.reshape(-1).tolist()
+
+
 def _pcg32(state: int):
     state = (state * 6364136223846793005 + 11634580027462260723) & _M64
     xorshifted = (((state >> 18) ^ state) >> 27) & _M32
@@ -81,10 +123,14 @@ class ChaCha20Rng:
             words.append(x)
         return cls(struct.pack("<8I", *words))
 
+    # keystream blocks generated per refill: the words come out in the same
+    # order whatever the refill size (blocks depend only on key and counter)
+    REFILL_BLOCKS = 64
+
     def next_u32(self) -> int:
         if not self.buf:
-            self.buf = chacha20_block(self.key, self.counter)
-            self.counter += 1
+            self.buf = chacha20_blocks(self.key, self.counter, self.REFILL_BLOCKS)
+            self.counter += self.REFILL_BLOCKS
             self.buf.reverse()
         return self.buf.pop()
 
