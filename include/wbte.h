@@ -295,7 +295,10 @@ int32_t wbte_wbtx_verify_shares_many(wbte_ctx *ctx, int32_t *ok, const wbte_wbtx
  * 11 * 32 affine G2 points ([m 64^w] vk, 67,584 bytes each), party-major.
  * Given to verify_shares_many as vk_tables (NULL: Pippenger over the keys),
  * each aggregate takes one mixed addition per nonzero signed radix-64 digit
- * of the challenges' base-|x| digits and no doublings. */
+ * of the challenges' base-|x| digits and no doublings.  The tables must have
+ * been built for the same party_indices, in the same order, and the same
+ * batch_size as the verify_shares_many call: the call reads T * batch_size
+ * tables and cannot check the buffer it is given. */
 int32_t wbte_wbtx_vk_tables(wbte_ctx *ctx, void *tables, const wbte_wbtx_key *key, const int64_t *party_indices,
                             uint64_t T, uint64_t batch_size);
 int32_t wbte_wbtx_precompute_many(wbte_ctx *ctx, void *beta, const void *kernel_lines, const void *first,
