@@ -149,7 +149,7 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: str):
         self.device = device
         self.proc = None
         self.path = None
@@ -407,7 +407,14 @@ def main():
     if args.warmup:  # correctness gate (untimed)
         assert wb.to_host(out, 576 * B) == b"".join(plain_p[args.warmup - 1])
     launches0 = _lib.load().wbte_ctx_launch_count(None)
-    sampler = ClockSampler(local)
+    # nvidia-smi numbers GPUs physically; CUDA_VISIBLE_DEVICES may renumber
+    # them for CUDA, so the sampler names this rank's GPU by its UUID
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        gpu_id = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+    except (AttributeError, RuntimeError):
+        gpu_id = str(local)
+    sampler = ClockSampler(gpu_id)
     barrier()
     torch.cuda.synchronize()
     sampler.start()
