@@ -225,3 +225,26 @@ def test_group_of_32_batches_matches_one_by_one():
     out = serving.decrypt_group(dk, [wb.CiphertextBatch.upload(c) for c in batches], keys,
                                 ChaCha20Rng.seed_from_u64(3), serving.CommitteeCache(1 << 30))
     assert out == msgs
+
+
+def test_group_with_a_dishonest_party_matches_one_by_one():
+    """A party whose shares are well-formed points but wrong fails every
+    batch's aggregate share check: the group decryption blames that share in
+    each batch and decrypts with the honest remainder, exactly as each batch
+    alone does."""
+    import dataclasses
+
+    rng = ChaCha20Rng.seed_from_u64(31)
+    mat = wb.keygen_with_rng(wb.KeygenConfig(8, [3, 2, 4, 1], 4), rng)
+    dk = mat.decryption_key
+    bad = dataclasses.replace(mat.party_keys[1], _q=(mat.party_keys[1].secret_scalar() + 1) % wb.R)
+    keys = [mat.party_keys[0], bad, mat.party_keys[2]]  # 0 and 2 alone carry weight 7 > 4
+    batches = []
+    for _ in range(3):
+        msgs = wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(8)])
+        batches.append(wb.encrypt_many(mat.encryption_key, msgs, rng))
+    cache = serving.CommitteeCache(1 << 30)
+    grouped = serving.decrypt_group(dk, batches, keys, ChaCha20Rng.seed_from_u64(5), cache)
+    alone = [serving.decrypt_request(dk, cts, keys, ChaCha20Rng.seed_from_u64(5), cache) for cts in batches]
+    assert grouped == alone
+    assert all(r is not None for res in grouped for r in res)
