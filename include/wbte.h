@@ -95,10 +95,11 @@ int32_t wbte_g2_msm(wbte_ctx *ctx, void *out, const void *points, const void *sc
  * Working memory is one fixed 8 MiB array in the library's device image,
  * held by every GPU that loads the library until the process exits; the
  * call allocates nothing and needs no context.
- *   - out, points, scalars: device memory of the current device (host
- *     pointers are rejected with WBTE_ERR_INVALID_ARG); stream: a
- *     cudaStream_t (NULL: legacy default stream).  Asynchronous.
- *   - n <= 16384 points; larger n returns WBTE_ERR_SIZE.
+ *   - out, points, scalars: device memory of the current device (host,
+ *     managed and other GPUs' pointers are rejected with
+ *     WBTE_ERR_INVALID_ARG); stream: a cudaStream_t (NULL: legacy default
+ *     stream).  Asynchronous.
+ *   - n <= 16384 points (every such n runs; larger n returns WBTE_ERR_SIZE).
  *   - The first call on a device looks up the array's device address (with
  *     that device current); make that first call before any stream capture.
  *   - Every call shares the array and it keeps the last call's contents:

@@ -17,8 +17,8 @@
  * `p{1,2}s_mult_pippenger` scalar format).
  *
  * Algorithms restated from the reference (paths inside the reference project):
- *   - hard part of the final exponentiation: btx/src/final_exponentiation.rs:308-336
- *     (raise_to_z / raise_to_z_div_by_2 at :451-466)
+  *   - hard part of the final exponentiation: btx/src/final_exponentiation.rs:255-283
+  *     (raise_to_z / raise_to_z_div_by_2 at :399-413)
  *   - easy part and batched easy part: btx/src/final_exponentiation.rs:276-305,356-371
  *   - Radix-2 DIT transform with bit reversal: btx/src/fft.rs:357-411,584-595
  *   - truncated cyclotomic inverse transform: btx/src/fft.rs:284-350

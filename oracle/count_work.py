@@ -10,7 +10,7 @@ products (products and squares, each counted once) it performs:
   weight), weighted_btx/src/decryption.rs:463-506;
 * the truncated cyclotomic inverse transform of the cross-term
   precomputation (m = 1024 values, first 512 outputs), btx/src/fft.rs:284-350;
-* one hard final exponentiation, btx/src/final_exponentiation.rs:308-336.
+* one hard final exponentiation, btx/src/final_exponentiation.rs:255-283.
 
     python -m oracle.count_work      # writes weighted_bte_b200/algorithmic_work.json
 

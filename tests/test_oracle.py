@@ -26,7 +26,7 @@ def test_reference_constants_pin_the_curve(orc, consts):
 
 
 def test_hard_part_is_the_reference_chain(orc, consts):
-    """The addition chain of btx/src/final_exponentiation.rs:308-336 raises to 3h."""
+    """The addition chain of btx/src/final_exponentiation.rs:255-283 raises to 3h."""
     h = sum(l << (64 * i) for i, l in enumerate(consts["hard_exponent_limbs_le"]))
     f = orc.easy_final_exp(orc.miller_loop(orc.g1_mul(orc.g1_generator(), 5), orc.g2_mul(orc.g2_generator(), 9)))
     assert orc.hard_final_exp(f) == orc.fp12_pow(f, 3 * h)

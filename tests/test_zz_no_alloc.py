@@ -30,9 +30,11 @@ def test_static_msm_matches_the_allocating_entry_point_on_consecutive_calls():
     torch.cuda.set_device(0)
     lib = _lib.load()
     rng = random.Random(4242)
-    # two calls in a row through the C ABI: the second reuses the array that
-    # still holds the first call's intermediates
-    for n in (3000, 517):
+    # calls in a row through the C ABI, each reusing the array that still
+    # holds the previous call's intermediates: the documented maximum, sizes
+    # that the allocating entry point sends to its small-MSM kernel (n <= 4),
+    # and sizes in between
+    for n in (16384, 3000, 517, 4, 1):
         points = ops.g1_mul_generator([rng.randrange(ops.R) for _ in range(n)])
         scalars = ops.scalars_bytes([rng.randrange(ops.R) for _ in range(n)])
         expect = ops.g1_msm(points, scalars)  # the existing, allocating entry point

@@ -376,24 +376,44 @@ static __device__ __align__(256) uint8_t g_static_msm_scratch[STATIC_MSM_BYTES];
 std::mutex g_static_mu;
 uint8_t* g_static_addr[128] = {};
 
-bool static_is_device(const void* p) {
+// Plain device memory of device `dev` only: host, managed and other GPUs'
+// memory are rejected (a peer pointer would be read over the interconnect).
+bool static_is_device(const void* p, int dev) {
     cudaPointerAttributes a;
     if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
+// The plan of wbte_g1_msm with fewer, longer segments where its scratch would
+// not fit the array: every n <= STATIC_MSM_MAX_POINTS fits (at n = 16384 the
+// digits and sorted entries take 3.6 MB and at most about 1000 segments of
+// the 22 windows fit the rest).
+bool static_plan(wbte::MsmPlan& p, int64_t n, size_t avail) {
+    using namespace wbte;
+    p = msm_plan(GROUP_G1, n, 1);
+    while (msm_family_scratch_bytes(GROUP_G1, 1, 1, n, p) > avail) {
+        if (p.segments <= 1) return false;
+        p.segment += std::max<int64_t>(1, p.segment / 8);
+        p.segments = (n + p.segment - 1) / p.segment;
+    }
+    return true;
 }
 }  // namespace
 
 extern "C" int32_t wbte_g1_msm_static(void* out, const void* points, const void* scalars, uint64_t n, void* stream) {
     using namespace wbte;
     if (n > STATIC_MSM_MAX_POINTS) return -2;  // WBTE_ERR_SIZE
-    if (!static_is_device(out) || (n > 0 && (!static_is_device(points) || !static_is_device(scalars))))
-        return -1;  // WBTE_ERR_INVALID_ARG: device pointers only
-    cudaStream_t s = (cudaStream_t)stream;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return -5;  // WBTE_ERR_CUDA
+    if (!static_is_device(out, dev) || (n > 0 && (!static_is_device(points, dev) || !static_is_device(scalars, dev))))
+        return -1;  // WBTE_ERR_INVALID_ARG: device pointers of the current device only
+    cudaStream_t s = (cudaStream_t)stream;
+    // an error left pending by earlier, unrelated runtime calls on this
+    // thread must not be reported as this call's failure
+    cudaGetLastError();
     uint8_t* base = nullptr;
     {
         // one-time set-up per device, with that device current
@@ -409,9 +429,8 @@ extern "C" int32_t wbte_g1_msm_static(void* out, const void* points, const void*
         base = g_static_addr[dev];
     }
     if (n == 0) return cudaMemsetAsync(out, 0, G1_AFF, s) == cudaSuccess ? 0 : -5;
-    MsmPlan p = msm_plan(GROUP_G1, (int64_t)n, 1);
-    size_t need = msm_family_scratch_bytes(GROUP_G1, 1, 1, (int64_t)n, p);
-    if (need > STATIC_MSM_BYTES - STATIC_MSM_TAIL) return -2;
+    MsmPlan p;
+    if (!static_plan(p, (int64_t)n, STATIC_MSM_BYTES - STATIC_MSM_TAIL)) return -2;
     // point base of the single MSM: zero (the tail of the array is reused by
     // every call, so it is cleared here; nothing else must start at zero)
     int64_t* pbase = reinterpret_cast<int64_t*>(base + STATIC_MSM_BYTES - STATIC_MSM_TAIL);

@@ -10,7 +10,7 @@
 // canonical, so this scaling is free to differ from any other implementation.
 //
 // The hard part follows the addition chain of the reference,
-// btx/src/final_exponentiation.rs:308-336 (with raise_to_z at :451-466),
+// btx/src/final_exponentiation.rs:255-283 (with raise_to_z at :399-413),
 // which computes f^(3 (p^4 - p^2 + 1) / r).
 #pragma once
 #include "curves.cuh"

@@ -256,24 +256,41 @@ def decrypt_group(dk: wb.PublicDecryptionKey, batches: Sequence, party_keys: Seq
         accepted = [wb.finish_acceptance(dk, validated[b], *screened[b], bool(ok[b])) for b in range(K)]
     else:
         accepted = [wb.accept_decryption_shares(dk, validated[b], shares[b], rng) for b in range(K)]
-    committees = {tuple(a.party_indices()) for a in accepted}
-    if len(committees) != 1:  # a share was rejected in some batch: decrypt those one by one
-        return [decrypt_request(dk, cts, party_keys, rng, cache, device_output) for cts in batches]
-    pre = cache.get(dk, accepted[0]) if cache is not None else wb.prepare_decryption(dk, accepted[0])
-    Ta = accepted[0].party_count()
-    sigmas = b"".join(s.sigma for a in accepted for s in a.shares())
-    second = torch.cat([c.second[: GTB * B] if isinstance(c, wb.CiphertextBatch)
-                        else wb.to_device(b"".join(x.second for x in c)) for c in batches])
-    out = wb.empty_device(GTB * B * K)
-    # precompute_batch and open_batch of all K batches, the cross terms and the
-    # opening pairings sharing one hard final exponentiation per slot
-    ctx.call("wbte_wbtx_decrypt_many", out, pre.kernel_lines, pre.opening_keys, pre.opening_lines, first, second,
-             valid, sigmas, Ta, B, K)
-    if device_output:
-        return [out[GTB * B * b : GTB * B * (b + 1)] for b in range(K)]
-    host = wb.to_host(out, GTB * B * K)
-    return [[host[GTB * (b * B + i) : GTB * (b * B + i + 1)] if validated[b].valid[i] else None for i in range(B)]
-            for b in range(K)]
+    # a batch whose share check blamed a party keeps its own (smaller)
+    # accepted committee: the batches are split by accepted committee and each
+    # part is decrypted as one group, so one bad share costs one extra group,
+    # not K single-batch decryptions
+    parts: "collections.OrderedDict[tuple, List[int]]" = collections.OrderedDict()
+    for b, a in enumerate(accepted):
+        parts.setdefault(tuple(a.party_indices()), []).append(b)
+    second_all = torch.cat([c.second[: GTB * B] if isinstance(c, wb.CiphertextBatch)
+                            else wb.to_device(b"".join(x.second for x in c)) for c in batches])
+    results: List = [None] * K
+    for idx in parts.values():
+        acc = [accepted[b] for b in idx]
+        pre = cache.get(dk, acc[0]) if cache is not None else wb.prepare_decryption(dk, acc[0])
+        Ta, Kp = acc[0].party_count(), len(idx)
+        sigmas = b"".join(s.sigma for a in acc for s in a.shares())
+        if Kp == K:
+            f_p, v_p, s_p = first, valid, second_all
+        else:
+            f_p = torch.cat([first[G1B * B * b : G1B * B * (b + 1)] for b in idx])
+            v_p = torch.cat([valid[B * b : B * (b + 1)] for b in idx])
+            s_p = torch.cat([second_all[GTB * B * b : GTB * B * (b + 1)] for b in idx])
+        out = wb.empty_device(GTB * B * Kp)
+        # precompute_batch and open_batch of the part's batches, the cross terms
+        # and the opening pairings sharing one hard final exponentiation per slot
+        ctx.call("wbte_wbtx_decrypt_many", out, pre.kernel_lines, pre.opening_keys, pre.opening_lines, f_p, s_p,
+                 v_p, sigmas, Ta, B, Kp)
+        if device_output:
+            for q, b in enumerate(idx):
+                results[b] = out[GTB * B * q : GTB * B * (q + 1)]
+        else:
+            host = wb.to_host(out, GTB * B * Kp)
+            for q, b in enumerate(idx):
+                results[b] = [host[GTB * (q * B + i) : GTB * (q * B + i + 1)] if validated[b].valid[i] else None
+                              for i in range(B)]
+    return results
 
 
 @dataclass
