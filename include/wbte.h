@@ -63,6 +63,21 @@ int32_t wbte_ctx_destroy(wbte_ctx *ctx);
  * stream; cudaStreamLegacy to order with the legacy default stream). */
 int32_t wbte_ctx_set_stream(wbte_ctx *ctx, void *cuda_stream);
 int32_t wbte_ctx_synchronize(wbte_ctx *ctx);
+/* Knobs of the launchers' cost models for every later call on this context
+ * (the per-size-class autotuner sets them; results never depend on them):
+ *   WBTE_TUNE_GT_LANES     lanes per GT exponentiation in the radix-4 stages
+ *                          of the GT transforms: 1, 2 or 4 (0: cost model)
+ *   WBTE_TUNE_MSM_WINDOW   Pippenger window width c, 4..13 (0: cost model)
+ *   WBTE_TUNE_MSM_SEGMENTS sorted-term segments per (MSM, window), 1..1024
+ *                          (0: cost model)
+ *   WBTE_TUNE_NTT_JOINT    G1/G2 transform stages: 1 one thread per
+ *                          butterfly, 0 the lane split (-1: cost model)
+ * WBTE_ERR_INVALID_ARG for an unknown knob or a value out of range. */
+#define WBTE_TUNE_GT_LANES 1
+#define WBTE_TUNE_MSM_WINDOW 2
+#define WBTE_TUNE_MSM_SEGMENTS 3
+#define WBTE_TUNE_NTT_JOINT 4
+int32_t wbte_ctx_set_tuning(wbte_ctx *ctx, int32_t knob, int64_t value);
 const char *wbte_ctx_last_error(const wbte_ctx *ctx);
 /* Number of kernels the library has launched so far (all contexts). */
 uint64_t wbte_ctx_launch_count(const wbte_ctx *ctx);
@@ -420,6 +435,48 @@ int32_t wbte_wpfe_open(wbte_ctx *ctx, void *messages, const void *sigmas, uint64
                        const void *first, const void *mask_lines, const void *first_cauchy,
                        const void *pairing_cauchy, const void *second, const void *alpha_products,
                        uint64_t B);
+
+/* The batched form: K batches of one (power-of-two) size B against one
+ * accepted committee per call, batch-major arrays (batch b first).  Each call
+ * is the K-fold version of the call above it with every kernel launched once
+ * over all K batches; per batch the results equal the single-batch call's.
+ *   partial_decrypt_many  sigma K*T G1 (sigma[b T + j] of party j in batch b),
+ *                         first K*B G1, rho T Fr, alpha B Fr
+ *   verify_shares_many    ok K int32 (one aggregate check per batch,
+ *                         weighted_pfe/src/decryption.rs:367-419), first K*B,
+ *                         sigma K*T, challenges K*T Fr, party_indices T (host),
+ *                         vk_tables from wbte_wpfe_vk_tables or NULL
+ *   precompute_many       first_cauchy K*B G1, pairing_cauchy K*B GT over the
+ *                         committee's B total line tables
+ *   open_many             messages K*B GT; sigmas K*T G1; by_party B*T G2
+ *                         (shared) and by_party_lines, their line tables
+ *                         (wbte_g2_prepare_lines of the B*T points) or NULL --
+ *                         with them each slot's T pairings share one
+ *                         multi-Miller loop (T <= 8); first, first_cauchy K*B
+ *                         G1; pairing_cauchy, second K*B GT; alpha_products B Fr
+ *   decrypt_many          precompute_many followed by open_many in one call
+ *                         (weighted_pfe/src/decryption.rs:540-644, the
+ *                         decrypt() of :646-669 after acceptance), without the
+ *                         intermediate outputs. */
+int32_t wbte_wpfe_partial_decrypt_many(wbte_ctx *ctx, void *sigma, const void *first, const void *rho,
+                                       const void *alpha, uint64_t T, uint64_t B, uint64_t K);
+/* Fixed-base tables of the verification keys of T parties at every slot
+ * (T * B tables, party-major, 67,584 bytes each), as wbte_wbtx_vk_tables. */
+int32_t wbte_wpfe_vk_tables(wbte_ctx *ctx, void *tables, const wbte_wpfe_key *key, const int64_t *party_indices,
+                            uint64_t T);
+int32_t wbte_wpfe_verify_shares_many(wbte_ctx *ctx, int32_t *ok, const wbte_wpfe_key *key, const void *first,
+                                     const void *sigma, const int64_t *party_indices, const void *challenges,
+                                     uint64_t T, uint64_t K, const void *vk_tables);
+int32_t wbte_wpfe_precompute_many(wbte_ctx *ctx, void *first_cauchy, void *pairing_cauchy, const void *first,
+                                  const void *total_lines, uint64_t B, uint64_t K);
+int32_t wbte_wpfe_open_many(wbte_ctx *ctx, void *messages, const void *sigmas, uint64_t T, const void *by_party,
+                            const void *by_party_lines, const void *first, const void *mask_lines,
+                            const void *first_cauchy, const void *pairing_cauchy, const void *second,
+                            const void *alpha_products, uint64_t B, uint64_t K);
+int32_t wbte_wpfe_decrypt_many(wbte_ctx *ctx, void *messages, const void *sigmas, uint64_t T, const void *by_party,
+                               const void *by_party_lines, const void *total_lines, const void *mask_lines,
+                               const void *first, const void *second, const void *alpha_products, uint64_t B,
+                               uint64_t K);
 
 /* ------------------------------------------------------------- pfe */
 /* PartialFractionKernel::new (pfe/src/decryption.rs:151-257) from the slot

@@ -31,6 +31,7 @@ STATUS_NAMES = {
     -8: "WBTE_ERR_INTERNAL",
 }
 FE_FULL, FE_EASY, FE_HARD = 0, 1, 2
+TUNE_GT_LANES, TUNE_MSM_WINDOW, TUNE_MSM_SEGMENTS, TUNE_NTT_JOINT = 1, 2, 3, 4
 CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 G1_BYTES, G2_BYTES, GT_BYTES, FR_BYTES, LINE_BYTES, MILLER_LINES = 96, 192, 576, 32, 288, 68
 FIXED_TABLE_BYTES = 192 * 11 * 32  # fixed-base table of one G2 point (wbte_wbtx_vk_tables)
@@ -147,6 +148,12 @@ _SIGNATURES = {
     "wbte_wbtx_precompute_many": [_VP, _VP, _VP, _VP, _U64, _U64],
     "wbte_wbtx_open_many": [_VP, _VP, _VP, _VP, _U64, _VP, _VP, _VP, _U64, _U64],
     "wbte_wbtx_decrypt_many": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64, _U64],
+    "wbte_wpfe_partial_decrypt_many": [_VP, _VP, _VP, _VP, _U64, _U64, _U64],
+    "wbte_wpfe_vk_tables": [_VP, _VP, _VP, _U64],
+    "wbte_wpfe_verify_shares_many": [_VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64, _VP],
+    "wbte_wpfe_precompute_many": [_VP, _VP, _VP, _VP, _U64, _U64],
+    "wbte_wpfe_open_many": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64],
+    "wbte_wpfe_decrypt_many": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64],
     "wbte_pfe_kernel": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
     "wbte_pfe_precompute": [_VP, _VP, _VP, _VP, _VP, _U64],
     "wbte_pfe_open": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64],
@@ -155,7 +162,7 @@ EXPORTED = sorted(
     list(_SIGNATURES)
     + ["wbte_version", "wbte_ctx_create", "wbte_ctx_destroy", "wbte_ctx_set_stream", "wbte_ctx_synchronize",
        "wbte_ctx_last_error", "wbte_ctx_launch_count", "wbte_profile_enable", "wbte_profile_read",
-       "wbte_g1_msm_static"]
+       "wbte_g1_msm_static", "wbte_ctx_set_tuning"]
 )
 
 
@@ -204,6 +211,8 @@ def load():
         lib.wbte_ctx_destroy.restype = _I32
         lib.wbte_ctx_set_stream.argtypes = [_VP, _VP]
         lib.wbte_ctx_set_stream.restype = _I32
+        lib.wbte_ctx_set_tuning.argtypes = [_VP, _I32, _I64]
+        lib.wbte_ctx_set_tuning.restype = _I32
         lib.wbte_ctx_synchronize.argtypes = [_VP]
         lib.wbte_ctx_synchronize.restype = _I32
         lib.wbte_ctx_last_error.argtypes = [_VP]
@@ -304,6 +313,10 @@ class Context:
 
     def synchronize(self):
         self._check(self.lib.wbte_ctx_synchronize(self.handle))
+
+    def set_tuning(self, knob: int, value: int):
+        """One knob of the launchers' cost models (TUNE_*) for later calls."""
+        self._check(self.lib.wbte_ctx_set_tuning(self.handle, int(knob), int(value)))
 
     def launch_count(self) -> int:
         return int(self.lib.wbte_ctx_launch_count(self.handle))

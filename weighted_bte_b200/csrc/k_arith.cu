@@ -904,9 +904,10 @@ void launch_negate(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStre
 // thread's Fp products (G1: 128 doublings and 66 additions joint, against 128
 // and 33 per lane on 2 lanes; G2: 64 and 68 against 64 and 17 per lane on 4
 // lanes) times max(1, threads / resident threads).  WBTE_NTT_JOINT = 0 or 1
-// overrides the choice.
+// overrides the choice, and so does the calling context's tuning knob.
 static bool ntt_joint(Group g, int64_t butterflies) {
     if (const char* env = getenv("WBTE_NTT_JOINT")) return atoi(env) != 0;
+    if (g_tune.ntt_joint == 0 || g_tune.ntt_joint == 1) return g_tune.ntt_joint == 1;
     static std::atomic<int64_t> cap[2][2] = {{{0}, {0}}, {{0}, {0}}};
     const int gi = g == GROUP_G1 ? 0 : 1;
     int64_t c[2];

@@ -331,13 +331,15 @@ __global__ void __launch_bounds__(WARP, WBTE_GT_MINBLOCKS) k_gt_pow(uint8_t* out
 // for all four digits on one lane, about 52 with the warp-uniform NAF plan
 // of k_gt_radix4_pows_plan; 65 and 40 on each of two; 65 and 25 on each of
 // four, with the Frobenius maps and the lane combine) times
-// max(1, E L / resident threads).  WBTE_GT_LANES = 1, 2 or 4 overrides it.
+// max(1, E L / resident threads).  WBTE_GT_LANES = 1, 2 or 4 overrides it, and
+// so does the calling context's tuning knob.
 static int gt_pow_lanes(int64_t E, bool shared_plan) {
     static std::atomic<int64_t> cap{0};
     if (const char* env = getenv("WBTE_GT_LANES")) {
         const int v = atoi(env);
         if (v == 1 || v == 2 || v == 4) return v;
     }
+    if (g_tune.gt_lanes == 1 || g_tune.gt_lanes == 2 || g_tune.gt_lanes == 4) return g_tune.gt_lanes;
     int64_t c = cap.load();
     if (c == 0) {
         int dev = 0, sms = 0, blocks = 0;

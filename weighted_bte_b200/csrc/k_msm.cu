@@ -288,6 +288,7 @@ MsmPlan msm_plan(Group g, int64_t n, int64_t k) {
     if (n >= (1 << 14)) c = lg - 2;
     if (c < 4) c = 4;
     if (c > 13) c = 13;
+    if (g_tune.msm_window >= 4 && g_tune.msm_window <= 13) c = g_tune.msm_window;
     p.c = c;
     p.windows = (256 + c - 1) / c;
     p.buckets = 1 << (c - 1);
@@ -313,6 +314,7 @@ MsmPlan msm_plan(Group g, int64_t n, int64_t k) {
             best_s = s;
         }
     }
+    if (g_tune.msm_segments > 0) best_s = std::min<int64_t>(std::min<int64_t>(g_tune.msm_segments, 1024), n);
     p.segment = (n + best_s - 1) / best_s;
     p.segments = (n + p.segment - 1) / p.segment;
     if (p.segments < 1) p.segments = 1;
@@ -393,7 +395,10 @@ bool static_is_device(const void* p, int dev) {
 // the 22 windows fit the rest).
 bool static_plan(wbte::MsmPlan& p, int64_t n, size_t avail) {
     using namespace wbte;
+    const Tuning saved = g_tune;
+    g_tune = Tuning();
     p = msm_plan(GROUP_G1, n, 1);
+    g_tune = saved;
     while (msm_family_scratch_bytes(GROUP_G1, 1, 1, n, p) > avail) {
         if (p.segments <= 1) return false;
         p.segment += std::max<int64_t>(1, p.segment / 8);

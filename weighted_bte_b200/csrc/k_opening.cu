@@ -13,14 +13,16 @@ inline unsigned blocks_for(int64_t n, int tpb = TPB) { return (unsigned)((n + tp
 
 WBTE_INL Fp12* as_gt(uint8_t* p) { return reinterpret_cast<Fp12*>(p); }
 
-// out[o] = prod_{t < T} Miller(P[(o / per) * T + t], lines of table (o % per) * T + t):
+// out[o] = prod_{t < T} Miller(P[(o / p_per) * T + t], lines of table (o % per) * T + t):
 // the opening of K batches against one committee's prepared opening keys
-// (tables line-major with stride per * T), each batch with its own T shares.
+// (tables line-major with stride per * T), each batch with its own T shares
+// (p_per = per: weighted_btx) or each slot with its own T points (p_per = 1:
+// weighted_pfe).
 __global__ void k_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per,
-                                     int T) {
+                                     int64_t p_per, int T) {
     int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (o >= n) return;
-    const int64_t b = o / per, i = o % per;
+    const int64_t b = o / p_per, i = o % per;
     Fp12 f;
     multi_miller_loop_lines(f, reinterpret_cast<const Line*>(lines) + i * T, (size_t)(per * T), 1,
                             reinterpret_cast<const G1A*>(p) + b * T, T);
@@ -30,12 +32,12 @@ __global__ void k_miller_lines_multi(uint8_t* out, const uint8_t* lines, const u
 }  // namespace
 
 bool launch_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per, int T,
-                               cudaStream_t s) {
+                               cudaStream_t s, int64_t p_per) {
     ProfScope prof_("miller_lines_multi", s);
-    if (T < 1 || T > MULTI_MILLER_MAX) return false;
+    if (T < 1 || T > MULTI_MILLER_MAX || per < 1) return false;
     if (n <= 0) return true;
     note_launch();
-    k_miller_lines_multi<<<blocks_for(n), TPB, 0, s>>>(out, lines, p, n, per, T);
+    k_miller_lines_multi<<<blocks_for(n), TPB, 0, s>>>(out, lines, p, n, per, p_per > 0 ? p_per : per, T);
     return true;
 }
 

@@ -27,6 +27,18 @@ struct ProfScope {
     ~ProfScope() { prof_end(token, s); }
 };
 
+// Knobs of the launchers' cost models for the library call running on this
+// thread (0 / -1: the cost model decides).  Each ABI call copies its
+// context's knobs (wbte_ctx_set_tuning) here for its duration; the
+// per-size-class autotuner measures candidate values through them.
+struct Tuning {
+    int gt_lanes = 0;      // lanes per GT exponentiation in the radix-4 transform stages: 1, 2 or 4
+    int msm_window = 0;    // Pippenger window width c, 4..13
+    int msm_segments = 0;  // sorted-term segments per (MSM, window), 1..1024
+    int ntt_joint = -1;    // G1/G2 transform stages: 1 one thread per butterfly, 0 the lane split
+};
+extern thread_local Tuning g_tune;
+
 constexpr size_t G1_AFF = 96, G2_AFF = 192, G1_XYZZ = 192, G2_XYZZ = 384, GT_SZ = 576, FR_SZ = 32;
 constexpr size_t LINE_SZ = 288;  // three Fp2 coefficients
 constexpr int LINES_PER_POINT = 68;
@@ -115,11 +127,12 @@ void launch_msm_family_scratch(Group g, uint8_t* out, const uint8_t* points, con
 // lines[step * n + i] for step < 68: prepared line coefficients of q[i]
 void launch_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n, cudaStream_t s);
 // out[i] = Miller(p[i], lines of pair i), lines laid out as above with n pairs
-// out[o] = prod_{t<T} Miller(p[(o / per) T + t], line table (o % per) T + t) for o < n
-// (tables line-major, stride per * T); returns false when T exceeds the
-// supported pair count (8), launching nothing.
+// out[o] = prod_{t<T} Miller(p[(o / p_per) T + t], line table (o % per) T + t) for o < n
+// (tables line-major, stride per * T; p_per <= 0 means per); returns false
+// when T exceeds the supported pair count (8), launching nothing.
+constexpr int MULTI_MILLER_MAX_PAIRS = 8;  // pairs per multi-Miller loop of launch_miller_lines_multi
 bool launch_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per, int T,
-                               cudaStream_t s);
+                               cudaStream_t s, int64_t p_per = 0);
 void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, cudaStream_t s,
                          int64_t lines_n = 0);
 // out[i] = Miller(p[p_mod ? i % p_mod : i], q[i])

@@ -29,6 +29,7 @@ std::atomic<bool> g_prof_on{false};
 }  // namespace
 
 thread_local bool g_prof_suppress = false;
+thread_local Tuning g_tune;
 
 void prof_begin(const char* tag, cudaStream_t s, void** token) {
     *token = nullptr;
@@ -58,6 +59,7 @@ struct wbte_ctx {
     std::string err;
     std::map<std::pair<int64_t, int>, uint8_t*> twiddles;
     std::mutex mu;
+    Tuning tune;
 };
 
 namespace {
@@ -99,7 +101,15 @@ struct Call {
     int32_t status = WBTE_OK;
     bool sync = false;
 
-    explicit Call(wbte_ctx* c) : ctx(c), s(c->stream) { cudaSetDevice(c->device); }
+    Tuning saved_tune;
+
+    explicit Call(wbte_ctx* c) : ctx(c), s(c->stream), saved_tune(g_tune) {
+        cudaSetDevice(c->device);
+        g_tune = c->tune;
+    }
+    ~Call() { g_tune = saved_tune; }
+    Call(const Call&) = delete;
+    Call& operator=(const Call&) = delete;
 
     int32_t fail(int32_t code, const std::string& msg) {
         if (status == WBTE_OK) {
@@ -343,6 +353,32 @@ int32_t wbte_ctx_set_stream(wbte_ctx* ctx, void* stream) {
     if (!ctx) return WBTE_ERR_INVALID_ARG;
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
     return WBTE_OK;
+}
+
+int32_t wbte_ctx_set_tuning(wbte_ctx* ctx, int32_t knob, int64_t value) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    switch (knob) {
+    case WBTE_TUNE_GT_LANES:
+        if (value != 0 && value != 1 && value != 2 && value != 4) break;
+        ctx->tune.gt_lanes = (int)value;
+        return WBTE_OK;
+    case WBTE_TUNE_MSM_WINDOW:
+        if (value != 0 && (value < 4 || value > 13)) break;
+        ctx->tune.msm_window = (int)value;
+        return WBTE_OK;
+    case WBTE_TUNE_MSM_SEGMENTS:
+        if (value < 0 || value > 1024) break;
+        ctx->tune.msm_segments = (int)value;
+        return WBTE_OK;
+    case WBTE_TUNE_NTT_JOINT:
+        if (value < -1 || value > 1) break;
+        ctx->tune.ntt_joint = (int)value;
+        return WBTE_OK;
+    default:
+        break;
+    }
+    ctx->err = "unknown tuning knob or value out of range";
+    return WBTE_ERR_INVALID_ARG;
 }
 
 int32_t wbte_ctx_synchronize(wbte_ctx* ctx) {
@@ -1375,116 +1411,268 @@ int32_t wbte_wpfe_prepare(wbte_ctx* ctx, const wbte_wpfe_key* key, const int64_t
     return c.finish();
 }
 
-int32_t wbte_wpfe_precompute(wbte_ctx* ctx, void* first_cauchy, void* pairing_cauchy, const void* first,
-                             const void* total_lines, uint64_t B) {
-    if (!ctx) return WBTE_ERR_INVALID_ARG;
-    Call c(ctx);
-    if (!first_cauchy || !pairing_cauchy || !first || !total_lines || B == 0)
-        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
-    if (log2_exact(B) < 0) return c.fail(WBTE_ERR_SIZE, "batch size must be a power of two");
-    uint8_t* dfc = c.out(first_cauchy, G1_AFF * B);
-    uint8_t* dpc = c.out(pairing_cauchy, GT_SZ * B);
-    const uint8_t* dfirst = c.in(first, G1_AFF * B);
-    const uint8_t* dl = c.in(total_lines, LINE_SZ * LINES_PER_POINT * B);
-    // closed-form Cauchy spectrum B - 1 - 2k (weighted_pfe/src/decryption.rs:194-213)
-    std::vector<int64_t> coeff(B);
-    std::vector<int32_t> rot(B);
-    for (uint64_t k = 0; k < B; k++) {
-        coeff[k] = (int64_t)B - 1 - 2 * (int64_t)k;
-        rot[k] = (int32_t)((k + B - 1) % B);
-    }
+// The Cauchy sums of K batches of one size B laid back to back
+// (precompute_batch, weighted_pfe/src/decryption.rs:540-574, :683-734):
+//   dfc[b B + i] = 2B sum_{k != i} first[b B + k] / (alpha_k - alpha_i)
+//   dpc[b B + i] = the same sums over e(first[b B + k], total_k) on easy-final-
+//                  exponentiated values (canonical after the hard part),
+// with the closed-form spectrum B - 1 - 2k of the Cauchy kernel (:194-213):
+// per batch a forward transform, the spectrum, a cyclic rotation by one and
+// the inverse transform, every step one launch over all K batches.
+static bool wpfe_precompute_core(Call& c, uint8_t* dfc, uint8_t* dpc, const uint8_t* dfirst, const uint8_t* dl,
+                                 uint64_t B, uint64_t K) {
+    const uint64_t n = B * K;
+    std::vector<int64_t> coeff(n);
+    std::vector<int32_t> rot(n);
+    for (uint64_t b = 0; b < K; b++)
+        for (uint64_t k = 0; k < B; k++) {
+            coeff[b * B + k] = (int64_t)B - 1 - 2 * (int64_t)k;
+            rot[b * B + k] = (int32_t)(b * B + (k + B - 1) % B);
+        }
     const uint8_t* dcoef = c.in_vec(fr_small_signed(coeff));
     const int32_t* drot = c.in_vec(rot);
-    uint8_t* x = c.alloc(G1_AFF * B);
-    uint8_t* y = c.alloc(G1_AFF * B);
-    uint8_t* work = c.alloc(G1_XYZZ * B);
-    uint8_t* f = c.alloc(GT_SZ * B);
-    uint8_t* h = c.alloc(GT_SZ * B);
+    uint8_t* x = c.alloc(G1_AFF * n);
+    uint8_t* y = c.alloc(G1_AFF * n);
+    uint8_t* work = c.alloc(G1_XYZZ * n);
+    uint8_t* f = c.alloc(GT_SZ * n);
+    uint8_t* h = c.alloc(GT_SZ * n);
     const uint8_t* tw = B > 1 ? twiddles(c, (int64_t)B, false) : nullptr;
     const uint8_t* twi = B > 1 ? twiddles(c, (int64_t)B, true) : nullptr;
-    if (!c.ok()) return c.finish();
+    if (!c.ok()) return false;
     // G1: 2B sum_{k != i} first_k / (alpha_k - alpha_i) (:683-708)
-    cudaMemcpyAsync(x, dfirst, G1_AFF * B, cudaMemcpyDeviceToDevice, c.s);
-    if (B > 1) launch_group_ntt(GROUP_G1, x, work, tw, (int64_t)B, c.s);
-    launch_mul_batch(GROUP_G1, y, x, 1, dcoef, (int64_t)B, c.s);
-    launch_gather(x, y, drot, (int64_t)B, G1_AFF, c.s);
-    launch_negate(GROUP_G1, x, x, (int64_t)B, c.s);
-    if (B > 1) launch_group_ntt(GROUP_G1, x, work, twi, (int64_t)B, c.s);
-    cudaMemcpyAsync(dfc, x, G1_AFF * B, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpyAsync(x, dfirst, G1_AFF * n, cudaMemcpyDeviceToDevice, c.s);
+    if (B > 1) launch_group_ntt(GROUP_G1, x, work, tw, (int64_t)B, c.s, (int64_t)K);
+    launch_mul_batch(GROUP_G1, y, x, 1, dcoef, (int64_t)n, c.s);
+    launch_gather(x, y, drot, (int64_t)n, G1_AFF, c.s);
+    launch_negate(GROUP_G1, x, x, (int64_t)n, c.s);
+    if (B > 1) launch_group_ntt(GROUP_G1, x, work, twi, (int64_t)B, c.s, (int64_t)K);
+    cudaMemcpyAsync(dfc, x, G1_AFF * n, cudaMemcpyDeviceToDevice, c.s);
     // GT: the same sums over e(first_k, D1_k) on easy-final-exponentiated values (:710-734)
-    launch_miller_lines(f, dl, dfirst, (int64_t)B, c.s);
-    launch_final_exp(f, f, (int64_t)B, FE_EASY, c.s);
-    if (B > 1) launch_gt_ntt(f, tw, (int64_t)B, c.s);
-    launch_gt_pow(h, f, 1, dcoef, (int64_t)B, c.s);
-    launch_gather(f, h, drot, (int64_t)B, GT_SZ, c.s);
-    launch_fp12_conj(f, f, (int64_t)B, c.s);
-    if (B > 1) launch_gt_ntt(f, twi, (int64_t)B, c.s, 1, true);
-    cudaMemcpyAsync(dpc, f, GT_SZ * B, cudaMemcpyDeviceToDevice, c.s);
-    return c.finish();
+    launch_miller_lines(f, dl, dfirst, (int64_t)n, c.s, (int64_t)B);
+    launch_final_exp(f, f, (int64_t)n, FE_EASY, c.s);
+    if (B > 1) launch_gt_ntt(f, tw, (int64_t)B, c.s, (int64_t)K);
+    launch_gt_pow(h, f, 1, dcoef, (int64_t)n, c.s);
+    launch_gather(f, h, drot, (int64_t)n, GT_SZ, c.s);
+    launch_fp12_conj(f, f, (int64_t)n, c.s);
+    if (B > 1) launch_gt_ntt(f, twi, (int64_t)B, c.s, (int64_t)K, true);
+    cudaMemcpyAsync(dpc, f, GT_SZ * n, cudaMemcpyDeviceToDevice, c.s);
+    return true;
+}
+
+// The opening of K batches of one size B against one committee
+// (open_batch, weighted_pfe/src/decryption.rs:576-644):
+//   messages[b B + i] = second - hard(e(first_i, mask_i) /
+//       (prod_k e(2B sigma_{b,k} - first_cauchy_i, by_party[i T + k]) pairing_cauchy_i)^(alpha_i (alpha_i + 1)))
+// ds: K*T shares (batch-major); dby: B*T G2 (shared); by_lines: their line
+// tables or NULL (then T unprepared loops per slot); dap: B Fr.
+static bool wpfe_open_core(Call& c, uint8_t* dm, const uint8_t* ds, uint64_t T, const uint8_t* dby,
+                           const void* by_lines, const uint8_t* dfirst, const uint8_t* dml, const uint8_t* dfc,
+                           const uint8_t* dpc, const uint8_t* d2, const uint8_t* dap, uint64_t B, uint64_t K) {
+    const uint64_t n = B * K, nt = n * T;
+    const uint8_t* d2b = c.in_vec(fr_small_signed(std::vector<int64_t>(T * K, 2 * (int64_t)B)));
+    std::vector<int32_t> idx_share(nt), idx_slot(nt), idx_ap(n);
+    // segment offsets carry k + 1 entries for k segments
+    std::vector<int64_t> offs_2(nt + 1);
+    for (uint64_t o = 0; o < n; o++) {
+        idx_ap[o] = (int32_t)(o % B);
+        for (uint64_t k = 0; k < T; k++) {
+            idx_share[o * T + k] = (int32_t)((o / B) * T + k);
+            idx_slot[o * T + k] = (int32_t)o;
+        }
+    }
+    for (uint64_t x = 0; x <= nt; x++) offs_2[x] = (int64_t)(2 * x);
+    const int32_t* dis = c.in_vec(idx_share);
+    const int32_t* dil = c.in_vec(idx_slot);
+    const int32_t* dia = c.in_vec(idx_ap);
+    const int64_t* do2 = c.in_vec(offs_2);
+    uint8_t* scaled = c.alloc(G1_AFF * T * K);
+    uint8_t* negfc = c.alloc(G1_AFF * n);
+    uint8_t* g0 = c.alloc(G1_AFF * nt);
+    uint8_t* g1 = c.alloc(G1_AFF * nt);
+    uint8_t* pairs = c.alloc(2 * G1_AFF * nt);
+    uint8_t* left = c.alloc(G1_AFF * nt);
+    uint8_t* ft = c.alloc(GT_SZ * n);
+    uint8_t* mp = c.alloc(GT_SZ * n);
+    uint8_t* apr = c.alloc(FR_SZ * n);
+    const bool prepared = by_lines && T <= (uint64_t)MULTI_MILLER_MAX_PAIRS;
+    const uint8_t* dbl = prepared ? c.in(by_lines, LINE_SZ * LINES_PER_POINT * B * T) : nullptr;
+    uint8_t* f = c.alloc(GT_SZ * (prepared ? n : nt));
+    if (!c.ok()) return false;
+    // left[(b B + i) T + k] = 2B sigma_{b,k} - first_cauchy[b B + i] (:596-612)
+    launch_mul_batch(GROUP_G1, scaled, ds, 1, d2b, (int64_t)(T * K), c.s);
+    launch_negate(GROUP_G1, negfc, dfc, (int64_t)n, c.s);
+    launch_gather(g0, scaled, dis, (int64_t)nt, G1_AFF, c.s);
+    launch_gather(g1, negfc, dil, (int64_t)nt, G1_AFF, c.s);
+    cudaMemcpy2DAsync(pairs, 2 * G1_AFF, g0, G1_AFF, G1_AFF, nt, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(pairs + G1_AFF, 2 * G1_AFF, g1, G1_AFF, G1_AFF, nt, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(GROUP_G1, left, pairs, do2, (int64_t)nt, c.s);
+    // first terms: per slot the T pairings with the committee's keys of that
+    // slot, one multi-Miller loop over their line tables when given
+    if (prepared) {
+        launch_miller_lines_multi(ft, dbl, left, (int64_t)n, (int64_t)B, (int)T, c.s, 1);
+    } else {
+        std::vector<int64_t> offs_T(n + 1);
+        for (uint64_t o = 0; o <= n; o++) offs_T[o] = (int64_t)(o * T);
+        const int64_t* doT = c.in_vec(offs_T);
+        if (!c.ok()) return false;
+        launch_miller(f, left, dby, (int64_t)nt, c.s, 0, (int64_t)(B * T));
+        launch_fp12_segment_product(ft, f, doT, (int64_t)n, c.s);
+    }
+    launch_miller_lines(mp, dml, dfirst, (int64_t)n, c.s, (int64_t)B);
+    launch_final_exp(ft, ft, (int64_t)n, FE_EASY, c.s);
+    launch_final_exp(mp, mp, (int64_t)n, FE_EASY, c.s);
+    // mask = hard(mp / (ft pairing_cauchy)^(alpha (alpha + 1))); message = second / mask (:614-643)
+    launch_fp12_mul(ft, ft, 1, dpc, 1, false, (int64_t)n, c.s);
+    launch_gather(apr, dap, dia, (int64_t)n, FR_SZ, c.s);
+    launch_gt_pow(f, ft, 1, apr, (int64_t)n, c.s);
+    launch_fp12_mul(mp, mp, 1, f, 1, true, (int64_t)n, c.s);
+    launch_final_exp(mp, mp, (int64_t)n, FE_HARD, c.s);
+    launch_fp12_mul(dm, d2, 1, mp, 1, true, (int64_t)n, c.s);
+    return true;
+}
+
+int32_t wbte_wpfe_precompute(wbte_ctx* ctx, void* first_cauchy, void* pairing_cauchy, const void* first,
+                             const void* total_lines, uint64_t B) {
+    return wbte_wpfe_precompute_many(ctx, first_cauchy, pairing_cauchy, first, total_lines, B, 1);
 }
 
 int32_t wbte_wpfe_open(wbte_ctx* ctx, void* messages, const void* sigmas, uint64_t T, const void* by_party,
                        const void* first, const void* mask_lines, const void* first_cauchy, const void* pairing_cauchy,
                        const void* second, const void* alpha_products, uint64_t B) {
+    return wbte_wpfe_open_many(ctx, messages, sigmas, T, by_party, nullptr, first, mask_lines, first_cauchy,
+                               pairing_cauchy, second, alpha_products, B, 1);
+}
+
+// ------------------------------------------- weighted_pfe, K batches per call
+int32_t wbte_wpfe_partial_decrypt_many(wbte_ctx* ctx, void* sigma, const void* first, const void* rho,
+                                       const void* alpha, uint64_t T, uint64_t B, uint64_t K) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (T == 0 || K == 0) return c.finish();
+    if (!sigma || !first || !rho || !alpha || B == 0) return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    uint8_t* dsig = c.out(sigma, G1_AFF * T * K);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B * K);
+    const uint8_t* dr = c.in(rho, FR_SZ * T);
+    const uint8_t* da = c.in(alpha, FR_SZ * B);
+    uint8_t* g = c.alloc(FR_SZ * T * B);
+    std::vector<int64_t> base(T * K);
+    std::vector<int32_t> vsel(T * K);
+    for (uint64_t b = 0; b < K; b++)
+        for (uint64_t j = 0; j < T; j++) {
+            base[b * T + j] = (int64_t)(b * B);
+            vsel[b * T + j] = (int32_t)j;
+        }
+    const int64_t* db = c.in_vec(base);
+    const int32_t* dv = c.in_vec(vsel);
+    if (!c.ok()) return c.finish();
+    // sigma[b T + j] = sum_i g_{j,i} first[b B + i] (weighted_pfe/src/decryption.rs:231-252):
+    // the T fraction vectors are shared by the K batches' MSMs
+    launch_wpfe_fractions(g, nullptr, dr, da, nullptr, (int64_t)T, (int64_t)B, true, c.s);
+    launch_msm_family(GROUP_G1, dsig, dfirst, db, nullptr, g, dv, (int32_t)T, (int64_t)(T * K), (int64_t)B, c.s);
+    return c.finish();
+}
+
+static wbte_wbtx_key wpfe_as_wbtx_key(const wbte_wpfe_key* key) {
+    wbte_wbtx_key wk;
+    wk.domain_points = key->domain_points;
+    wk.verification_keys = key->verification_keys;
+    wk.negative_material = key->d1;
+    wk.positive_material = key->d2;
+    wk.party_offsets = key->party_offsets;
+    wk.party_count = key->party_count;
+    wk.total_weight = key->total_weight;
+    wk.max_batch_size = key->batch_size;
+    return wk;
+}
+
+int32_t wbte_wpfe_vk_tables(wbte_ctx* ctx, void* tables, const wbte_wpfe_key* key, const int64_t* party_indices,
+                            uint64_t T) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    {
+        Call c(ctx);
+        if (check_wpfe_key(c, key)) return c.finish();
+    }
+    wbte_wbtx_key wk = wpfe_as_wbtx_key(key);
+    return wbte_wbtx_vk_tables(ctx, tables, &wk, party_indices, T, key->batch_size);
+}
+
+int32_t wbte_wpfe_verify_shares_many(wbte_ctx* ctx, int32_t* ok, const wbte_wpfe_key* key, const void* first,
+                                     const void* sigma, const int64_t* party_indices, const void* challenges,
+                                     uint64_t T, uint64_t K, const void* vk_tables) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    {
+        Call c(ctx);
+        if (check_wpfe_key(c, key)) return c.finish();
+    }
+    // the aggregate check of verify_decryption_shares_batched
+    // (weighted_pfe/src/decryption.rs:367-419) per batch: weighted_pfe
+    // accepts a batch only when every proof holds, so every slot enters
+    wbte_wbtx_key wk = wpfe_as_wbtx_key(key);
+    return wbte_wbtx_verify_shares_many(ctx, ok, &wk, first, key->batch_size, sigma, party_indices, challenges, T, K,
+                                        vk_tables);
+}
+
+int32_t wbte_wpfe_precompute_many(wbte_ctx* ctx, void* first_cauchy, void* pairing_cauchy, const void* first,
+                                  const void* total_lines, uint64_t B, uint64_t K) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!first_cauchy || !pairing_cauchy || !first || !total_lines || B == 0 || K == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    if (log2_exact(B) < 0) return c.fail(WBTE_ERR_SIZE, "batch size must be a power of two");
+    uint8_t* dfc = c.out(first_cauchy, G1_AFF * B * K);
+    uint8_t* dpc = c.out(pairing_cauchy, GT_SZ * B * K);
+    const uint8_t* dfirst = c.in(first, G1_AFF * B * K);
+    const uint8_t* dl = c.in(total_lines, LINE_SZ * LINES_PER_POINT * B);
+    if (c.ok()) wpfe_precompute_core(c, dfc, dpc, dfirst, dl, B, K);
+    return c.finish();
+}
+
+int32_t wbte_wpfe_open_many(wbte_ctx* ctx, void* messages, const void* sigmas, uint64_t T, const void* by_party,
+                            const void* by_party_lines, const void* first, const void* mask_lines,
+                            const void* first_cauchy, const void* pairing_cauchy, const void* second,
+                            const void* alpha_products, uint64_t B, uint64_t K) {
     if (!ctx) return WBTE_ERR_INVALID_ARG;
     Call c(ctx);
     if (!messages || !sigmas || T == 0 || !by_party || !first || !mask_lines || !first_cauchy || !pairing_cauchy ||
-        !second || !alpha_products || B == 0)
+        !second || !alpha_products || B == 0 || K == 0)
         return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
-    uint8_t* dm = c.out(messages, GT_SZ * B);
-    const uint8_t* ds = c.in(sigmas, G1_AFF * T);
+    const uint64_t n = B * K;
+    uint8_t* dm = c.out(messages, GT_SZ * n);
+    const uint8_t* ds = c.in(sigmas, G1_AFF * T * K);
     const uint8_t* dby = c.in(by_party, G2_AFF * B * T);
-    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint8_t* dfirst = c.in(first, G1_AFF * n);
     const uint8_t* dml = c.in(mask_lines, LINE_SZ * LINES_PER_POINT * B);
-    const uint8_t* dfc = c.in(first_cauchy, G1_AFF * B);
-    const uint8_t* dpc = c.in(pairing_cauchy, GT_SZ * B);
-    const uint8_t* d2 = c.in(second, GT_SZ * B);
+    const uint8_t* dfc = c.in(first_cauchy, G1_AFF * n);
+    const uint8_t* dpc = c.in(pairing_cauchy, GT_SZ * n);
+    const uint8_t* d2 = c.in(second, GT_SZ * n);
     const uint8_t* dap = c.in(alpha_products, FR_SZ * B);
-    const uint8_t* d2b = c.in_vec(fr_small_signed(std::vector<int64_t>(T, 2 * (int64_t)B)));
-    std::vector<int32_t> idx_share(B * T), idx_slot(B * T);
-    // segment offsets carry k + 1 entries for k segments
-    std::vector<int64_t> offs_T(B + 1), offs_2(B * T + 1);
-    for (uint64_t i = 0; i < B; i++)
-        for (uint64_t k = 0; k < T; k++) {
-            idx_share[i * T + k] = (int32_t)k;
-            idx_slot[i * T + k] = (int32_t)i;
-        }
-    for (uint64_t x = 0; x <= B * T; x++) offs_2[x] = (int64_t)(2 * x);
-    for (uint64_t i = 0; i <= B; i++) offs_T[i] = (int64_t)(i * T);
-    const int32_t* dis = c.in_vec(idx_share);
-    const int32_t* dil = c.in_vec(idx_slot);
-    const int64_t* doT = c.in_vec(offs_T);
-    const int64_t* do2 = c.in_vec(offs_2);
-    uint8_t* scaled = c.alloc(G1_AFF * T);
-    uint8_t* negfc = c.alloc(G1_AFF * B);
-    uint8_t* g0 = c.alloc(G1_AFF * B * T);
-    uint8_t* g1 = c.alloc(G1_AFF * B * T);
-    uint8_t* pairs = c.alloc(2 * G1_AFF * B * T);
-    uint8_t* left = c.alloc(G1_AFF * B * T);
-    uint8_t* f = c.alloc(GT_SZ * B * T);
-    uint8_t* ft = c.alloc(GT_SZ * B);
-    uint8_t* mp = c.alloc(GT_SZ * B);
-    if (!c.ok()) return c.finish();
-    // left[i T + k] = 2B sigma_k - scaled_first_cauchy[i] (weighted_pfe/src/decryption.rs:596-612)
-    launch_mul_batch(GROUP_G1, scaled, ds, 1, d2b, (int64_t)T, c.s);
-    launch_negate(GROUP_G1, negfc, dfc, (int64_t)B, c.s);
-    launch_gather(g0, scaled, dis, (int64_t)(B * T), G1_AFF, c.s);
-    launch_gather(g1, negfc, dil, (int64_t)(B * T), G1_AFF, c.s);
-    cudaMemcpy2DAsync(pairs, 2 * G1_AFF, g0, G1_AFF, G1_AFF, B * T, cudaMemcpyDeviceToDevice, c.s);
-    cudaMemcpy2DAsync(pairs + G1_AFF, 2 * G1_AFF, g1, G1_AFF, G1_AFF, B * T, cudaMemcpyDeviceToDevice, c.s);
-    launch_segment_sum(GROUP_G1, left, pairs, do2, (int64_t)(B * T), c.s);
-    // first terms: per-slot multi-Miller loops over the T parties; mask pairings
-    launch_miller(f, left, dby, (int64_t)(B * T), c.s);
-    launch_fp12_segment_product(ft, f, doT, (int64_t)B, c.s);
-    launch_miller_lines(mp, dml, dfirst, (int64_t)B, c.s);
-    launch_final_exp(ft, ft, (int64_t)B, FE_EASY, c.s);
-    launch_final_exp(mp, mp, (int64_t)B, FE_EASY, c.s);
-    // mask = hard(mp / (ft pairing_cauchy)^(alpha (alpha + 1))); message = second / mask (:614-643)
-    launch_fp12_mul(ft, ft, 1, dpc, 1, false, (int64_t)B, c.s);
-    launch_gt_pow(f, ft, 1, dap, (int64_t)B, c.s);
-    launch_fp12_mul(mp, mp, 1, f, 1, true, (int64_t)B, c.s);
-    launch_final_exp(mp, mp, (int64_t)B, FE_HARD, c.s);
-    launch_fp12_mul(dm, d2, 1, mp, 1, true, (int64_t)B, c.s);
+    if (c.ok()) wpfe_open_core(c, dm, ds, T, dby, by_party_lines, dfirst, dml, dfc, dpc, d2, dap, B, K);
+    return c.finish();
+}
+
+int32_t wbte_wpfe_decrypt_many(wbte_ctx* ctx, void* messages, const void* sigmas, uint64_t T, const void* by_party,
+                               const void* by_party_lines, const void* total_lines, const void* mask_lines,
+                               const void* first, const void* second, const void* alpha_products, uint64_t B,
+                               uint64_t K) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!messages || !sigmas || T == 0 || !by_party || !total_lines || !mask_lines || !first || !second ||
+        !alpha_products || B == 0 || K == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    if (log2_exact(B) < 0) return c.fail(WBTE_ERR_SIZE, "batch size must be a power of two");
+    const uint64_t n = B * K;
+    uint8_t* dm = c.out(messages, GT_SZ * n);
+    const uint8_t* ds = c.in(sigmas, G1_AFF * T * K);
+    const uint8_t* dby = c.in(by_party, G2_AFF * B * T);
+    const uint8_t* dtl = c.in(total_lines, LINE_SZ * LINES_PER_POINT * B);
+    const uint8_t* dml = c.in(mask_lines, LINE_SZ * LINES_PER_POINT * B);
+    const uint8_t* dfirst = c.in(first, G1_AFF * n);
+    const uint8_t* d2 = c.in(second, GT_SZ * n);
+    const uint8_t* dap = c.in(alpha_products, FR_SZ * B);
+    uint8_t* fc = c.alloc(G1_AFF * n);
+    uint8_t* pc = c.alloc(GT_SZ * n);
+    if (c.ok() && wpfe_precompute_core(c, fc, pc, dfirst, dtl, B, K))
+        wpfe_open_core(c, dm, ds, T, dby, by_party_lines, dfirst, dml, fc, pc, d2, dap, B, K);
     return c.finish();
 }
 

@@ -98,30 +98,32 @@ class CommitteeCache:
         self.hits = 0
         self.misses = 0
 
-    def get(self, dk: wb.PublicDecryptionKey, accepted: wb.AcceptedDecryptionShares):
-        """Prepared committee for `accepted`, prepared on the calling thread's
-        current stream if absent.  The caller's stream is ordered after the
-        preparation."""
+    def obtain(self, key: bytes, build: Callable[[], tuple], count: bool = True):
+        """The value cached under `key`, built by `build()` on the calling
+        thread's current stream if absent.  build returns (value, tensors):
+        the device tensors the value holds, which count against the budget.
+        A thread that finds the value being built by another waits for it; the
+        caller's stream is ordered after the build (a CUDA event)."""
         torch = wb._t()
-        key = wb.decryption_context_id(dk.setup_id(), accepted.batch_size, accepted.party_indices())
         with self._lock:
             entry = self._entries.get(key)
             owner = entry is None
             if owner:
                 entry = _Entry()
                 self._entries[key] = entry
-                self.misses += 1
+                if count:
+                    self.misses += 1
             else:
                 self._entries.move_to_end(key)
-                self.hits += 1
+                if count:
+                    self.hits += 1
         if owner:
             try:
-                entry.pre = wb.prepare_decryption(dk, accepted)
+                value, tensors = build()
                 ev = torch.cuda.Event()
                 ev.record(torch.cuda.current_stream())
-                entry.ready = ev
-                entry.nbytes = sum(t.numel() for t in (entry.pre.kernel_lines, entry.pre.opening_keys,
-                                                        entry.pre.opening_lines, entry.pre.transformed_kernel))
+                entry.pre, entry.ready = (value, list(tensors)), ev
+                entry.nbytes = sum(t.numel() for t in tensors)
             except BaseException as exc:  # noqa: BLE001 -- handed to every waiter
                 entry.error = exc
                 with self._lock:
@@ -136,52 +138,38 @@ class CommitteeCache:
             raise entry.error
         stream = torch.cuda.current_stream()
         stream.wait_event(entry.ready)
-        for t in (entry.pre.kernel_lines, entry.pre.opening_keys, entry.pre.opening_lines,
-                  entry.pre.transformed_kernel):
+        value, tensors = entry.pre
+        for t in tensors:
             t.record_stream(stream)
-        return entry.pre
+        return value
+
+    def get(self, dk: wb.PublicDecryptionKey, accepted: wb.AcceptedDecryptionShares):
+        """Prepared committee for `accepted`, prepared on the calling thread's
+        current stream if absent.  The caller's stream is ordered after the
+        preparation."""
+        key = wb.decryption_context_id(dk.setup_id(), accepted.batch_size, accepted.party_indices())
+
+        def build():
+            pre = wb.prepare_decryption(dk, accepted)
+            return pre, [pre.kernel_lines, pre.opening_keys, pre.opening_lines, pre.transformed_kernel]
+
+        return self.obtain(key, build)
 
     def vk_tables(self, dk: wb.PublicDecryptionKey, batch_size: int, party_indices: Sequence[int]):
         """Fixed-base tables of the parties' verification keys at slots
         1..batch_size (wbte_wbtx_vk_tables), built once per party set and
         batch size on the calling thread's current stream; the share check of
         every later group of the same parties uses them."""
-        torch = wb._t()
         key = b"vk-tables" + dk.setup_id() + struct.pack("<Q", batch_size) + b"".join(
             struct.pack("<q", j) for j in party_indices)
-        with self._lock:
-            entry = self._entries.get(key)
-            owner = entry is None
-            if owner:
-                entry = _Entry()
-                self._entries[key] = entry
-            else:
-                self._entries.move_to_end(key)
-        if owner:
-            try:
-                T = len(party_indices)
-                tables = wb.empty_device(_lib.FIXED_TABLE_BYTES * T * batch_size)
-                wb._ctx().call("wbte_wbtx_vk_tables", tables, dk.abi_key(), _lib.i64_array(party_indices), T,
-                               batch_size)
-                ev = torch.cuda.Event()
-                ev.record(torch.cuda.current_stream())
-                entry.pre, entry.ready, entry.nbytes = tables, ev, tables.numel()
-            except BaseException as exc:  # noqa: BLE001 -- handed to every waiter
-                entry.error = exc
-                with self._lock:
-                    self._entries.pop(key, None)
-            finally:
-                entry.done.set()
-            if entry.error is None:
-                self._evict()
-        else:
-            entry.done.wait()
-        if entry.error is not None:
-            raise entry.error
-        stream = torch.cuda.current_stream()
-        stream.wait_event(entry.ready)
-        entry.pre.record_stream(stream)
-        return entry.pre
+
+        def build():
+            T = len(party_indices)
+            tables = wb.empty_device(_lib.FIXED_TABLE_BYTES * T * batch_size)
+            wb._ctx().call("wbte_wbtx_vk_tables", tables, dk.abi_key(), _lib.i64_array(party_indices), T, batch_size)
+            return tables, [tables]
+
+        return self.obtain(key, build, count=False)
 
     def _evict(self):
         with self._lock:

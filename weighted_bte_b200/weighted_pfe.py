@@ -431,6 +431,80 @@ def validate_batch(encryption_key: EncryptionKey, ciphertexts: Sequence[Cipherte
                           wb.to_device(first))
 
 
+def _device_arrays(cts):
+    """(first, commitment, second, responses) of one batch as device arrays
+    (first three) and host ints; `cts` is a list of Ciphertext or a
+    weighted_btx.CiphertextBatch (same fields, already in HBM)."""
+    if isinstance(cts, wb.CiphertextBatch):
+        n = len(cts)
+        return cts.first[: G1B * n], cts.commitment[: G1B * n], cts.second[: GTB * n], list(cts.responses)
+    return (wb.to_device(b"".join(c.first for c in cts)), wb.to_device(b"".join(c.proof.commitment for c in cts)),
+            wb.to_device(b"".join(c.second for c in cts)), [c.proof.response for c in cts])
+
+
+def validate_batches(encryption_key: EncryptionKey, batches: Sequence, rng=None, arrays=None) -> list:
+    """`validate_batch` for K batches of the key's batch size in one pass on
+    the device: every ciphertext's encodings and Fiat-Shamir challenge in one
+    launch each, and the K random-linear Schnorr aggregates
+    (weighted_pfe/src/proof.rs:74-122) as one family of K G1 MSMs of 2B + 1
+    terms.  Entry b is the ValidatedBatch of batch b, or the error that
+    validate_batch raises for it alone (a batch is rejected as a whole).
+    `arrays`: the batches' _device_arrays when the caller has them already."""
+    torch = wb._t()
+    K = len(batches)
+    if K == 0:
+        return []
+    B = encryption_key.batch_size()
+    out: list = [None] * K
+    live = []
+    for b, cts in enumerate(batches):
+        if len(cts) == 0:
+            out[b] = E.BatchIsEmpty()
+        elif len(cts) != B:
+            out[b] = E.MismatchedBatchSize(B, len(cts))
+        else:
+            live.append(b)
+    if not live:
+        return out
+    arrays = [arrays[b] if arrays is not None else _device_arrays(batches[b]) for b in live]
+    n = B * len(live)
+    first_all = torch.cat([a[0] for a in arrays])
+    comm_all = torch.cat([a[1] for a in arrays])
+    second_all = torch.cat([a[2] for a in arrays])
+    responses = [r for a in arrays for r in a[3]]
+    fc, te, cc = wb._encode_on_device(first_all, comm_all, second_all, n)
+    prefix = TRANSCRIPT_DOMAIN + encryption_key.setup_id() + ops.g1_compress(wb.g1_generator(), 1)
+    ch = ops.transcript_challenges([(prefix, 0, len(prefix), _lib.TRANSCRIPT_BYTES),
+                                    (fc, 48, 48, _lib.TRANSCRIPT_BYTES),
+                                    (struct.pack("<Q", 289), 0, 8, _lib.TRANSCRIPT_BYTES),
+                                    (te, 289, 289, _lib.TRANSCRIPT_BYTES),
+                                    (cc, 48, 48, _lib.TRANSCRIPT_BYTES)], n)
+    rng = rng or OsRng()
+    scalars = []
+    for q in range(len(live)):
+        coef = [sample_nonzero(rng) for _ in range(B)]
+        resp = responses[q * B : (q + 1) * B]
+        chq = ch[q * B : (q + 1) * B]
+        gen_s = sum(a * r for a, r in zip(coef, resp)) % R
+        scalars += [gen_s] + [(-a) % R for a in coef] + [(-a * c) % R for a, c in zip(coef, chq)]
+    g = wb.to_device(wb.g1_generator())
+    pts = torch.cat([t for q in range(len(live))
+                     for t in (g[:G1B], comm_all[G1B * B * q : G1B * B * (q + 1)],
+                               first_all[G1B * B * q : G1B * B * (q + 1)])])
+    n1 = 2 * B + 1
+    agg = ops.msm_family(1, pts, n1 * len(live), [q * n1 for q in range(len(live))], None, scalars,
+                         list(range(len(live))), len(live), n1)
+    rec = wb._records_host(fc, te, cc, wb.to_device(ops.scalars_bytes(responses)), n)
+    for q, b in enumerate(live):
+        if agg[G1B * q : G1B * (q + 1)] != G1_IDENTITY:
+            out[b] = E.InvalidProof()
+            continue
+        body = struct.pack("<Q", B) + rec[q * B : (q + 1) * B].tobytes()
+        digest = hashlib.sha256(BATCH_DIGEST_DOMAIN + body).digest()
+        out[b] = ValidatedBatch(encryption_key.setup_id(), B, digest, first_all[G1B * B * q : G1B * B * (q + 1)])
+    return out
+
+
 @dataclass
 class DecryptionShare:
     party_index: int
@@ -461,6 +535,38 @@ def partial_decrypt_many(party_keys: Sequence[PartySecretKey], batch: ValidatedB
                    ops.scalars_bytes(alpha), T, B)
     return [DecryptionShare(pk.party_index, bytes(sig[G1B * j : G1B * (j + 1)]), batch.digest(), batch.setup_id())
             for j, pk in enumerate(party_keys)]
+
+
+def partial_decrypt_batches(party_keys: Sequence[PartySecretKey], batches: Sequence[ValidatedBatch]):
+    """`partial_decrypt` of every party for K validated batches of one size in
+    one launch sequence (wbte_wpfe_partial_decrypt_many): shares[b][j] is party
+    j's share of batch b, equal to partial_decrypt(party_keys[j], batches[b])."""
+    torch = wb._t()
+    K = len(batches)
+    if K == 0 or not party_keys:
+        return [[] for _ in range(K)]
+    B = batches[0].batch_size()
+    for bt in batches:
+        if bt.batch_size() != B:
+            raise E.MismatchedBatchSize(B, bt.batch_size())
+        for pk in party_keys:
+            if pk.setup_id() != bt.setup_id():
+                raise E.MismatchedSetup()
+    for pk in party_keys:
+        if pk.batch_size() != B:
+            raise E.MismatchedBatchSize(pk.batch_size(), B)
+    T = len(party_keys)
+    alpha = [(r + party_keys[0].alpha_shift_small) % R for r in root_domain_prefix(B, B)]
+    for pk in party_keys:
+        if any((pk.rho + a) % R == 0 for a in alpha):
+            raise E.InvalidSecretKey()
+    first = torch.cat([bt.first_dev[: G1B * B] for bt in batches])
+    sig = bytearray(G1B * T * K)
+    wb._ctx().call("wbte_wpfe_partial_decrypt_many", sig, first, ops.scalars_bytes([pk.rho for pk in party_keys]),
+                   ops.scalars_bytes(alpha), T, B, K)
+    return [[DecryptionShare(pk.party_index, bytes(sig[G1B * (b * T + j) : G1B * (b * T + j + 1)]),
+                             batches[b].digest(), batches[b].setup_id()) for j, pk in enumerate(party_keys)]
+            for b in range(K)]
 
 
 def partial_decrypt(party_key: PartySecretKey, batch: ValidatedBatch) -> DecryptionShare:
@@ -522,6 +628,17 @@ def accept_decryption_shares(decryption_key: PublicDecryptionKey, batch: Validat
     """weighted_pfe/src/decryption.rs:277-365: batched check, per-share blame
     on failure, weight check, then the minimum-cardinality heaviest-first
     authorized subset."""
+    candidates, rejected = screen_shares(decryption_key, batch, shares)
+    rng = rng or OsRng()
+    ok = True
+    if candidates:
+        ok = _verify_shares(decryption_key, batch, candidates, [sample_nonzero(rng) for _ in candidates])
+    return finish_acceptance(decryption_key, batch, candidates, rejected, ok)
+
+
+def screen_shares(decryption_key: PublicDecryptionKey, batch: ValidatedBatch, shares: Sequence[DecryptionShare]):
+    """The structural checks of accept_decryption_shares (weighted_pfe/src/decryption.rs:277-300):
+    returns (candidates bound to this batch and setup, rejected party indices)."""
     _ensure_key_batch(decryption_key, batch)
     N = decryption_key.party_count()
     if len(shares) > N:
@@ -538,12 +655,17 @@ def accept_decryption_shares(decryption_key: PublicDecryptionKey, batch: Validat
             candidates.append(s)
         else:
             rejected.append(s.party_index)
-    rng = rng or OsRng()
-    ok = True
-    if candidates:
-        ok = _verify_shares(decryption_key, batch, candidates, [sample_nonzero(rng) for _ in candidates])
-    if ok:
-        valid = candidates
+    return candidates, rejected
+
+
+def finish_acceptance(decryption_key: PublicDecryptionKey, batch: ValidatedBatch, candidates, rejected,
+                      aggregate_ok: bool) -> AcceptedDecryptionShares:
+    """The rest of accept_decryption_shares (weighted_pfe/src/decryption.rs:300-365)
+    once the aggregate check has run: per-share blame on failure, weight check,
+    minimum heaviest-first authorized subset."""
+    rejected = list(rejected)
+    if aggregate_ok:
+        valid = list(candidates)
     else:
         valid = []
         for s in candidates:

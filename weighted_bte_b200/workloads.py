@@ -106,3 +106,70 @@ class WeightedBtxConfig:
 
 
 WBTX_B512 = WeightedBtxConfig("weighted_btx B=512 n=128 Zipf(1) W=4096 t=W/3", 512, 128, 4096, 1)
+
+
+def log_uniform_sizes(count: int, lo: int, hi: int, seed: int) -> List[int]:
+    """`count` batch sizes round(exp(U[ln lo, ln hi])) from a seeded stream."""
+    import math
+    import random
+
+    rng = random.Random(seed)
+    a, b = math.log(lo), math.log(hi)
+    return [min(hi, max(lo, int(round(math.exp(rng.uniform(a, b)))))) for _ in range(count)]
+
+
+@dataclass
+class WeightedPfeBatchedConfig:
+    """The batched form: `count` independent weighted_pfe batches with sizes
+    log-uniform in [lo, hi], padded to powers of two with valid dummy
+    encryptions; n parties with Zipf(1) weights scaled to W; threshold W/3."""
+
+    name: str
+    count: int
+    lo: int
+    hi: int
+    parties: int
+    total_weight: int
+    seed: int
+
+    @property
+    def weights(self) -> List[int]:
+        return zipf_weights(self.parties, self.total_weight)
+
+    @property
+    def threshold(self) -> int:
+        return self.total_weight // 3
+
+    def sizes(self) -> List[int]:
+        return log_uniform_sizes(self.count, self.lo, self.hi, self.seed)
+
+
+@dataclass
+class WeightedPfeServedConfig:
+    """The served form: requests of weighted_pfe batch decryption with sizes
+    log-uniform in [lo, hi] (padded to powers of two), n parties with
+    Pareto(alpha) weights scaled to W, threshold W/3, Poisson arrivals."""
+
+    name: str
+    lo: int
+    hi: int
+    parties: int
+    total_weight: int
+    alpha: float
+    seed: int
+
+    @property
+    def weights(self) -> List[int]:
+        return pareto_weights(self.parties, self.total_weight, self.alpha, self.seed)
+
+    @property
+    def threshold(self) -> int:
+        return self.total_weight // 3
+
+
+WPFE_BATCHED = WeightedPfeBatchedConfig(
+    "weighted_pfe batched: 256 batches, sizes log-uniform [8, 2048] padded to pow2, n=64 Zipf(1) W=2048 t=W/3",
+    256, 8, 2048, 64, 2048, 3)
+WPFE_SERVED = WeightedPfeServedConfig(
+    "weighted_pfe served: sizes log-uniform [16, 4096] padded to pow2, n=1000 Pareto(1.2) W=16384 t=W/3, "
+    "Poisson arrivals", 16, 4096, 1000, 16384, 1.2, 4)
