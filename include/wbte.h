@@ -298,7 +298,8 @@ int32_t wbte_wbtx_open(wbte_ctx *ctx, void *messages, const void *opening_keys, 
  *   open_many             messages K*B GT, opening_keys B*T G2 (shared),
  *                         opening_lines: their line tables (wbte_g2_prepare_lines
  *                         of the B*T keys) or NULL; with them each slot's T
- *                         pairings share one multi-Miller loop (T <= 8),
+ *                         pairings share one multi-Miller loop (in chunks of
+ *                         8 pairs),
  *                         sigma K*T G1, second/beta K*B GT, valid K*B. */
 int32_t wbte_wbtx_partial_decrypt_many(wbte_ctx *ctx, void *sigma, const void *first, uint64_t batch_size,
                                        const void *q, uint64_t T, uint64_t K);
@@ -452,7 +453,7 @@ int32_t wbte_wpfe_open(wbte_ctx *ctx, void *messages, const void *sigmas, uint64
  *                         (shared) and by_party_lines, their line tables
  *                         (wbte_g2_prepare_lines of the B*T points) or NULL --
  *                         with them each slot's T pairings share one
- *                         multi-Miller loop (T <= 8); first, first_cauchy K*B
+ *                         multi-Miller loop (in chunks of 8 pairs); first, first_cauchy K*B
  *                         G1; pairing_cauchy, second K*B GT; alpha_products B Fr
  *   decrypt_many          precompute_many followed by open_many in one call
  *                         (weighted_pfe/src/decryption.rs:540-644, the

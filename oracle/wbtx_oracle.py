@@ -12,6 +12,7 @@ seeded generator (weighted_bte_b200.rng) is only an input source here.
 """
 from __future__ import annotations
 
+import concurrent.futures as cf
 import hashlib
 import struct
 
@@ -140,8 +141,17 @@ def batch_digest(cts) -> bytes:
     return h.digest()
 
 
-def validate(setup_id, cts) -> dict:
-    valid = [verify_ct(setup_id, ct) for ct in cts]
+def _map(fn, items, threads: int):
+    """map on `threads` host threads (the C calls release the interpreter lock),
+    mirroring the reference's per-item rayon parallelism."""
+    if threads <= 1 or len(items) < 2:
+        return [fn(x) for x in items]
+    with cf.ThreadPoolExecutor(threads) as ex:
+        return list(ex.map(fn, items, chunksize=max(1, len(items) // (4 * threads))))
+
+
+def validate(setup_id, cts, threads: int = 1) -> dict:
+    valid = _map(lambda ct: verify_ct(setup_id, ct), list(cts), threads)
     first = [ct["first"] if v else O.G1_IDENTITY for ct, v in zip(cts, valid)]
     return dict(valid=valid, first=first, digest=batch_digest(cts), B=len(cts))
 
@@ -152,17 +162,13 @@ def partial_decrypt(q: int, batch: dict) -> bytes:
     return O.g1_msm(batch["first"], scalars)
 
 
-def verify_shares(key, batch, parties, sigmas, challenges) -> bool:
+def verify_shares(key, batch, parties, sigmas, challenges, threads: int = 1) -> bool:
     """weighted_btx/src/decryption.rs:358-422 with the given challenges."""
     agg = O.g1_msm(sigmas, challenges)
-    left, right = [], []
     N = key["N"]
-    for slot, v in enumerate(batch["valid"]):
-        if not v:
-            continue
-        bases = [key["vk"][slot * N + j] for j in parties]
-        right.append(O.g2_msm(bases, challenges))
-        left.append(batch["first"][slot])
+    slots = [slot for slot, v in enumerate(batch["valid"]) if v]
+    right = _map(lambda slot: O.g2_msm([key["vk"][slot * N + j] for j in parties], challenges), slots, threads)
+    left = [batch["first"][slot] for slot in slots]
     left.append(O.g1_neg(agg))
     right.append(O.g2_generator())
     f = O.multi_miller_many([(left, right)])[0]

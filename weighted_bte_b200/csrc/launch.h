@@ -128,9 +128,8 @@ void launch_msm_family_scratch(Group g, uint8_t* out, const uint8_t* points, con
 void launch_prepare_lines(uint8_t* lines, const uint8_t* q, int64_t n, cudaStream_t s);
 // out[i] = Miller(p[i], lines of pair i), lines laid out as above with n pairs
 // out[o] = prod_{t<T} Miller(p[(o / p_per) T + t], line table (o % per) T + t) for o < n
-// (tables line-major, stride per * T; p_per <= 0 means per); returns false
-// when T exceeds the supported pair count (8), launching nothing.
-constexpr int MULTI_MILLER_MAX_PAIRS = 8;  // pairs per multi-Miller loop of launch_miller_lines_multi
+// (tables line-major, stride per * T; p_per <= 0 means per); any T >= 1, the
+// pairs sharing their squarings in chunks of 8; returns false for T < 1.
 bool launch_miller_lines_multi(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, int64_t per, int T,
                                cudaStream_t s, int64_t p_per = 0);
 void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, int64_t n, cudaStream_t s,

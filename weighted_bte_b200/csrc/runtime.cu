@@ -1494,7 +1494,7 @@ static bool wpfe_open_core(Call& c, uint8_t* dm, const uint8_t* ds, uint64_t T, 
     uint8_t* ft = c.alloc(GT_SZ * n);
     uint8_t* mp = c.alloc(GT_SZ * n);
     uint8_t* apr = c.alloc(FR_SZ * n);
-    const bool prepared = by_lines && T <= (uint64_t)MULTI_MILLER_MAX_PAIRS;
+    const bool prepared = by_lines != nullptr;
     const uint8_t* dbl = prepared ? c.in(by_lines, LINE_SZ * LINES_PER_POINT * B * T) : nullptr;
     uint8_t* f = c.alloc(GT_SZ * (prepared ? n : nt));
     if (!c.ok()) return false;
@@ -2037,11 +2037,11 @@ int32_t wbte_wbtx_precompute_many(wbte_ctx* ctx, void* beta, const void* kernel_
 // alpha[b B + i] = prod_t Miller(sigma[b T + t], opening_keys[i T + t]) before
 // the final exponentiation (weighted_btx/src/decryption.rs:607-695): one
 // multi-Miller loop per slot over the prepared opening keys when their line
-// tables are given (T <= 8), else T unprepared loops and their product
+// tables are given, else T unprepared loops and their product
 static bool opening_miller(Call& c, uint8_t* alpha, const uint8_t* dk, const void* opening_lines, const uint8_t* ds,
                            uint64_t T, uint64_t B, uint64_t K) {
     const uint64_t BT = B * T;
-    if (opening_lines && T <= 8) {
+    if (opening_lines) {
         const uint8_t* dl = c.in(opening_lines, LINE_SZ * LINES_PER_POINT * BT);
         if (!c.ok()) return false;
         launch_miller_lines_multi(alpha, dl, ds, (int64_t)(B * K), (int64_t)B, (int)T, c.s);

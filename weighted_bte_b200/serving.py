@@ -281,6 +281,30 @@ def decrypt_group(dk: wb.PublicDecryptionKey, batches: Sequence, party_keys: Seq
     return results
 
 
+class WbtxBackend:
+    """How the server runs weighted_btx requests: memory estimate, grouping
+    key, and the decryption of a group (one request alone, or several of
+    one batch size and committee as one batched group)."""
+
+    def __init__(self, decryption_key: wb.PublicDecryptionKey):
+        self.dk = decryption_key
+
+    def need(self, ciphertexts, party_keys) -> int:
+        B, T = len(ciphertexts), len(party_keys)
+        # whether the committee will be cached is known only when the request
+        # runs, so admission always reserves room for preparing it
+        wt = sum(self.dk.party_weight(k.party_index) for k in party_keys)
+        return request_bytes(B, T) + preparation_bytes(B, T, wt)
+
+    def group_key(self, ciphertexts, party_keys):
+        return len(ciphertexts), tuple(k.party_index for k in party_keys)
+
+    def run(self, group, rng, cache) -> list:
+        if len(group) == 1:
+            return [decrypt_request(self.dk, group[0].ciphertexts, group[0].party_keys, rng, cache)]
+        return decrypt_group(self.dk, [r.ciphertexts for r in group], group[0].party_keys, rng, cache)
+
+
 @dataclass
 class _Request:
     ciphertexts: object
@@ -289,20 +313,27 @@ class _Request:
     need: int
     future: cf.Future
     submitted: float
+    key: object = None
     started: float = 0.0
 
 
 class DecryptionServer:
     """Request loop with continuous batching over `slots` CUDA streams.
 
-    submit() returns a Future of the request's result (one Optional[bytes]
-    per slot, None where the ciphertext's proof failed).  Latency is measured
-    from submit() to the result being available on the host."""
+    submit() returns a Future of the request's result (for weighted_btx one
+    Optional[bytes] per slot, None where the ciphertext's proof failed; a
+    request the scheme rejects as a whole raises its error through the
+    future).  Latency is measured from submit() to the result being
+    available on the host.  `backend` selects the scheme (default: weighted_btx
+    under `decryption_key`; wpfe_batched.WpfeBackend serves weighted_pfe);
+    `cache` shares a committee cache between servers of the same keys."""
 
-    def __init__(self, decryption_key: wb.PublicDecryptionKey, slots: int = 4,
+    def __init__(self, decryption_key: Optional[wb.PublicDecryptionKey] = None, slots: int = 4,
                  hbm_budget_bytes: Optional[int] = None, cache_bytes: Optional[int] = None,
-                 device: Optional[int] = None, cache_committees: bool = True, max_group: int = 1):
+                 device: Optional[int] = None, cache_committees: bool = True, max_group: int = 1, backend=None,
+                 cache: Optional[CommitteeCache] = None):
         torch = wb._t()
+        self.backend = backend if backend is not None else WbtxBackend(decryption_key)
         self.dk = decryption_key
         self.device = torch.cuda.current_device() if device is None else device
         # requests of one batch size and committee that wait together are
@@ -312,8 +343,11 @@ class DecryptionServer:
             free, _total = torch.cuda.mem_get_info(self.device)
             hbm_budget_bytes = free // 2
         self.budget = int(hbm_budget_bytes)
-        self.cache = CommitteeCache(cache_bytes if cache_bytes is not None else self.budget // 4) \
-            if cache_committees else None
+        if cache is not None:
+            self.cache = cache  # shared with other servers of the same keys
+        else:
+            self.cache = CommitteeCache(cache_bytes if cache_bytes is not None else self.budget // 4) \
+                if cache_committees else None
         self._cv = threading.Condition()
         self._queue: "collections.deque[_Request]" = collections.deque()
         self._in_use = 0
@@ -328,18 +362,13 @@ class DecryptionServer:
             w.start()
 
     # ---------------------------------------------------------------- API
-    def submit(self, ciphertexts, party_keys: Sequence[wb.PartySecretKey], seed: int = 0) -> cf.Future:
-        B = len(ciphertexts)
-        T = len(party_keys)
-        need = request_bytes(B, T)
-        # whether the committee will be cached is known only when the request
-        # runs, so admission always reserves room for preparing it
-        wt = sum(self.dk.party_weight(k.party_index) for k in party_keys)
-        need_prep = preparation_bytes(B, T, wt)
-        if need + need_prep > self.budget:
-            raise MemoryError(f"request of {B} ciphertexts needs ~{need + need_prep} bytes, budget {self.budget}")
+    def submit(self, ciphertexts, party_keys: Sequence, seed: int = 0) -> cf.Future:
+        need = self.backend.need(ciphertexts, party_keys)
+        if need > self.budget:
+            raise MemoryError(f"request of {len(ciphertexts)} ciphertexts needs ~{need} bytes, budget {self.budget}")
         fut: cf.Future = cf.Future()
-        req = _Request(ciphertexts, list(party_keys), seed, need + need_prep, fut, time.perf_counter())
+        req = _Request(ciphertexts, list(party_keys), seed, need, fut, time.perf_counter(),
+                       self.backend.group_key(ciphertexts, party_keys))
         with self._cv:
             if self._closed:
                 raise RuntimeError("server is closed")
@@ -377,7 +406,7 @@ class DecryptionServer:
     # ------------------------------------------------------------ workers
     @staticmethod
     def _group_key(req: _Request):
-        return len(req.ciphertexts), tuple(k.party_index for k in req.party_keys)
+        return req.key
 
     def _admit(self) -> Optional[List[_Request]]:
         """Admit the head request once it fits the budget, then every waiting
@@ -431,11 +460,7 @@ class DecryptionServer:
             try:
                 rng = ChaCha20Rng.seed_from_u64(group[0].seed)
                 with torch.cuda.stream(stream):
-                    if len(group) == 1:
-                        outs = [decrypt_request(self.dk, group[0].ciphertexts, group[0].party_keys, rng, self.cache)]
-                    else:
-                        outs = decrypt_group(self.dk, [r.ciphertexts for r in group], group[0].party_keys, rng,
-                                             self.cache)
+                    outs = self.backend.run(group, rng, self.cache)
                 stream.synchronize()
                 done = time.perf_counter()
                 with self._cv:
@@ -443,7 +468,10 @@ class DecryptionServer:
                         self.latencies.append(done - req.submitted)
                         self.completed_ciphertexts += len(req.ciphertexts)
                 for req, out in zip(group, outs):
-                    req.future.set_result(out)
+                    if isinstance(out, BaseException):
+                        req.future.set_exception(out)
+                    else:
+                        req.future.set_result(out)
             except BaseException as exc:  # noqa: BLE001 -- reported through the futures
                 for req in group:
                     if not req.future.done():

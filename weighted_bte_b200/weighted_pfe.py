@@ -292,15 +292,21 @@ def keygen_with_rng(config: KeygenConfig, rng) -> KeyMaterial:
     target = _append_gt_fixed_many(element, 1)[0]
     h.update(struct.pack("<Q", len(target)))
     h.update(target)
-    h.update(ops.g2_compress(vk, B * N))
-    h.update(ops.g2_compress(d1, B * W))
-    h.update(ops.g2_compress(d2, B * W))
-    h.update(ops.g2_compress(V, 1))
+    for arr, count in ((vk, B * N), (d1, B * W), (d2, B * W), (V, 1)):
+        _hash_compressed_g2(h, arr, count)
     setup_id = h.digest()
     dk = PublicDecryptionKey(setup_id, B, t, W, domain, config.party_weights, offsets, evaluation_domain, alpha, shift,
                              vk, d1, d2, V)
     parties = [PartySecretKey(j, setup_id, B, shift, rho) for j, rho in enumerate(rhos)]
     return KeyMaterial(EncryptionKey(B, element, setup_id), dk, parties)
+
+
+def _hash_compressed_g2(h, points_dev, count: int, chunk: int = 1 << 20):
+    """h.update of the compressed encodings of `count` device G2 points, in
+    chunks (the key material of large classes runs to tens of GB)."""
+    for i in range(0, count, chunk):
+        n = min(chunk, count - i)
+        h.update(ops.g2_compress(points_dev[G2B * i : G2B * (i + n)], n))
 
 
 def keygen(batch_size: int, party_weights: Sequence[int], threshold_weight: int) -> KeyMaterial:

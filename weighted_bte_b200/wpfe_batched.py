@@ -78,10 +78,14 @@ def _committee(cache: Optional[CommitteeCache], dk, accepted) -> PreparedCommitt
     return cache.obtain(key, build)
 
 
+VK_TABLE_LIMIT = 1 << 30  # bytes of fixed-base verification-key tables per class and committee
+
+
 def _vk_tables(cache: Optional[CommitteeCache], dk, parties: Sequence[int]):
     """Fixed-base tables of the parties' verification keys at every slot
-    (wbte_wpfe_vk_tables), cached per setup and party set."""
-    if cache is None:
+    (wbte_wpfe_vk_tables), cached per setup and party set; None (the share
+    check's Pippenger path) without a cache or beyond VK_TABLE_LIMIT."""
+    if cache is None or _lib.FIXED_TABLE_BYTES * len(parties) * dk.batch_size() > VK_TABLE_LIMIT:
         return None
     key = b"wpfe-vk" + dk.setup_id() + b"".join(int(j).to_bytes(8, "little") for j in parties)
 
@@ -314,3 +318,55 @@ def _apply_knobs(ctx, knobs: dict):
     ctx.set_tuning(_lib.TUNE_MSM_WINDOW, int(knobs.get("msm_window", 0)))
     ctx.set_tuning(_lib.TUNE_MSM_SEGMENTS, int(knobs.get("msm_segments", 0)))
     ctx.set_tuning(_lib.TUNE_NTT_JOINT, int(knobs.get("ntt_joint", -1)))
+
+
+# ------------------------------------------------------------- served form
+def request_bytes(B: int, T: int) -> int:
+    """Device memory one weighted_pfe request of class B (committee of T)
+    holds while it runs: the batch and its encodings, the validation MSM, the
+    Cauchy transforms (G1 work, two GT arrays), the opening's per-(slot,
+    party) G1 points and GT values, and the output."""
+    return B * (6400 + 480 * T) + (1 << 20)
+
+
+def preparation_bytes(B: int, T: int) -> int:
+    """Device memory of one prepared committee of class B (kept in the cache)
+    plus the working memory of preparing it: per-party keys and their line
+    tables, the total and mask line tables, the verification-key tables
+    (when within VK_TABLE_LIMIT), the preparation's MSM scratch."""
+    tables = _lib.FIXED_TABLE_BYTES * T * B
+    tables = tables if tables <= VK_TABLE_LIMIT else 0
+    lines = _lib.LINE_BYTES * _lib.MILLER_LINES
+    return B * T * (G2B + lines + 32 * 2 * G2B) + 2 * B * lines + tables
+
+
+class WpfeBackend:
+    """Runs weighted_pfe requests in serving.DecryptionServer: a request is a
+    batch of any size s, routed to the class next_pow2(s), padded there with
+    the class's dummies and decrypted by the class's committee; requests of
+    one class and committee that wait together form one group
+    (`decrypt_group`).  A request's result is its s plaintexts; a batch the
+    scheme rejects raises that error through its future."""
+
+    def __init__(self, classes: Dict[int, SizeClass]):
+        self.classes = classes
+
+    def _class(self, ciphertexts) -> SizeClass:
+        B = size_class(len(ciphertexts))
+        if B not in self.classes:
+            raise E.InvalidBatchSize(B)
+        return self.classes[B]
+
+    def need(self, ciphertexts, party_keys) -> int:
+        sc = self._class(ciphertexts)
+        return request_bytes(sc.B, len(party_keys)) + preparation_bytes(sc.B, len(party_keys))
+
+    def group_key(self, ciphertexts, party_keys):
+        return size_class(len(ciphertexts)), tuple(k.party_index for k in party_keys)
+
+    def run(self, group, rng, cache) -> list:
+        sc = self._class(group[0].ciphertexts)
+        mat = sc.material
+        padded = [sc.pad(r.ciphertexts) for r in group]
+        outs = decrypt_group(mat.encryption_key, mat.decryption_key, padded, group[0].party_keys, rng, cache)
+        return [o[: len(r.ciphertexts)] if isinstance(o, list) else o for o, r in zip(outs, group)]
