@@ -151,6 +151,14 @@ int32_t wbte_g2_mul_generator(wbte_ctx *ctx, void *out, const void *scalars, uin
 /* out[j] = sum of in[offsets[j] .. offsets[j+1]) (offsets host, k+1 entries). */
 int32_t wbte_g1_sum(wbte_ctx *ctx, void *out, const void *in, const int64_t *offsets, uint64_t k);
 int32_t wbte_g2_sum(wbte_ctx *ctx, void *out, const void *in, const int64_t *offsets, uint64_t k);
+/* Projective to affine for n points (blst_p1s_to_affine / blst_p2s_to_affine
+ * as called by batch_normalize_g1/g2, weighted_btx/src/blst_utils.rs:11-36):
+ * in holds blst_p1 / blst_p2 records (Jacobian X, Y, Z; x = X/Z^2, y = Y/Z^3;
+ * 144 / 288 bytes), out affine points; Z = 0 gives the identity.  Chunks of
+ * consecutive points share one field inversion (Montgomery's trick).  out
+ * and in must not overlap. */
+int32_t wbte_g1_batch_normalize(wbte_ctx *ctx, void *out, const void *in, uint64_t n);
+int32_t wbte_g2_batch_normalize(wbte_ctx *ctx, void *out, const void *in, uint64_t n);
 /* ZCash compressed encodings, 48 / 96 bytes per point (to_compressed). */
 int32_t wbte_g1_compress(wbte_ctx *ctx, void *out, const void *in, uint64_t n);
 int32_t wbte_g2_compress(wbte_ctx *ctx, void *out, const void *in, uint64_t n);
@@ -478,6 +486,60 @@ int32_t wbte_wpfe_decrypt_many(wbte_ctx *ctx, void *messages, const void *sigmas
                                const void *by_party_lines, const void *total_lines, const void *mask_lines,
                                const void *first, const void *second, const void *alpha_products, uint64_t B,
                                uint64_t K);
+
+/* ---------------------------------------- resident keys and served form */
+/* A request loop in the library for callers without their own scheduler:
+ * validate ciphertexts and accept shares with the calls above (the crates'
+ * host logic), then submit each accepted batch's decryption -- precompute
+ * and open, the heavy part of decrypt() (weighted_btx/src/decryption.rs:555-709,
+ * weighted_pfe/src/decryption.rs:540-669) -- and poll for its messages.
+ *
+ * wbte_crs_upload_* copies one setup's public key material (host or device
+ * sources) into HBM owned by the handle; weighted_pfe also takes its 2 B
+ * mask scalars alpha_i (alpha_i + 1), then -alpha_i (as wbte_wpfe_prepare).
+ * A handle must outlive every server request that names it. */
+#define WBTE_SCHEME_WBTX 1
+#define WBTE_SCHEME_WPFE 2
+typedef struct wbte_crs wbte_crs;
+int32_t wbte_crs_upload_wbtx(wbte_ctx *ctx, const wbte_wbtx_key *key, wbte_crs **out);
+int32_t wbte_crs_upload_wpfe(wbte_ctx *ctx, const wbte_wpfe_key *key, const void *mask_scalars, wbte_crs **out);
+int32_t wbte_crs_destroy(wbte_crs *crs);
+
+typedef struct {
+    const wbte_crs *crs;          /* the setup (for weighted_pfe: the size class) */
+    uint64_t batch_size;          /* weighted_btx: <= the setup's maximum; weighted_pfe: the class size */
+    const void *first;            /* B G1 after validation (weighted_btx: identity at invalid slots) */
+    const void *second;           /* B GT */
+    const uint8_t *valid;         /* weighted_btx: B flags (NULL: all valid); weighted_pfe: ignored */
+    const void *sigma;            /* T G1: the accepted shares in party order */
+    const int64_t *party_indices; /* T accepted parties, ascending */
+    uint64_t party_count;         /* T */
+    void *messages;               /* out: B GT, host memory, written before the request completes */
+} wbte_request;
+
+typedef struct wbte_server wbte_server;
+/* `slots` worker threads on `device`, each with its own context and CUDA
+ * stream.  Waiting requests of one setup, batch size and committee are
+ * decrypted together, up to max_group batches per launch sequence (the
+ * _many calls); prepared committees stay cached in HBM for the server's
+ * lifetime; a request is admitted while the estimated device memory of the
+ * running groups stays within hbm_budget_bytes (0: half the free memory).
+ * Requests run in arrival order otherwise. */
+int32_t wbte_server_create(int32_t device, uint32_t slots, uint32_t max_group, uint64_t hbm_budget_bytes,
+                           wbte_server **out);
+/* Copies the request's inputs (the caller may reuse them on return) and
+ * queues it; *ticket names it for wbte_poll.  WBTE_ERR_OOM if the request
+ * alone exceeds the budget, WBTE_ERR_SIZE for a batch size its setup does
+ * not take. */
+int32_t wbte_submit(wbte_server *srv, const wbte_request *req, uint64_t *ticket);
+/* Waits at most timeout_ns for the request.  WBTE_ERR_TIMEOUT if it is still
+ * queued or running (the ticket stays valid); otherwise WBTE_OK, *status is
+ * the request's own status (its messages are written when it is WBTE_OK)
+ * and the ticket is released.  WBTE_ERR_INVALID_ARG for an unknown ticket. */
+int32_t wbte_poll(wbte_server *srv, uint64_t ticket, uint64_t timeout_ns, int32_t *status);
+/* Finishes every queued request, then stops the workers and frees the
+ * cached committees. */
+int32_t wbte_server_destroy(wbte_server *srv);
 
 /* ------------------------------------------------------------- pfe */
 /* PartialFractionKernel::new (pfe/src/decryption.rs:151-257) from the slot

@@ -74,6 +74,25 @@ class TranscriptField(ctypes.Structure):
 TRANSCRIPT_BYTES, TRANSCRIPT_GT_VARIABLE = 0, 1
 
 
+class Request(ctypes.Structure):
+    """wbte_request: one accepted batch submitted to a wbte_server."""
+
+    _fields_ = [
+        ("crs", ctypes.c_void_p),
+        ("batch_size", ctypes.c_uint64),
+        ("first", ctypes.c_void_p),
+        ("second", ctypes.c_void_p),
+        ("valid", ctypes.c_void_p),
+        ("sigma", ctypes.c_void_p),
+        ("party_indices", ctypes.c_void_p),
+        ("party_count", ctypes.c_uint64),
+        ("messages", ctypes.c_void_p),
+    ]
+
+
+SCHEME_WBTX, SCHEME_WPFE = 1, 2
+
+
 class WpfeKey(ctypes.Structure):
     _fields_ = [
         ("domain_points", ctypes.c_void_p),
@@ -101,6 +120,8 @@ _SIGNATURES = {
     "wbte_g2_mul_generator": [_VP, _VP, _U64],
     "wbte_g1_sum": [_VP, _VP, _VP, _U64],
     "wbte_g2_sum": [_VP, _VP, _VP, _U64],
+    "wbte_g1_batch_normalize": [_VP, _VP, _U64],
+    "wbte_g2_batch_normalize": [_VP, _VP, _U64],
     "wbte_g1_compress": [_VP, _VP, _U64],
     "wbte_g2_compress": [_VP, _VP, _U64],
     "wbte_g1_ntt": [_VP, _U64, _I32],
@@ -162,7 +183,8 @@ EXPORTED = sorted(
     list(_SIGNATURES)
     + ["wbte_version", "wbte_ctx_create", "wbte_ctx_destroy", "wbte_ctx_set_stream", "wbte_ctx_synchronize",
        "wbte_ctx_last_error", "wbte_ctx_launch_count", "wbte_profile_enable", "wbte_profile_read",
-       "wbte_g1_msm_static", "wbte_ctx_set_tuning"]
+       "wbte_g1_msm_static", "wbte_ctx_set_tuning", "wbte_crs_upload_wbtx", "wbte_crs_upload_wpfe",
+       "wbte_crs_destroy", "wbte_server_create", "wbte_submit", "wbte_poll", "wbte_server_destroy"]
 )
 
 
@@ -227,6 +249,17 @@ def load():
             fn = getattr(lib, name)
             fn.argtypes = [_VP] + args
             fn.restype = _I32
+        # resident keys and the served form
+        lib.wbte_crs_upload_wbtx.argtypes = [_VP, _VP, ctypes.POINTER(_VP)]
+        lib.wbte_crs_upload_wpfe.argtypes = [_VP, _VP, _VP, ctypes.POINTER(_VP)]
+        lib.wbte_crs_destroy.argtypes = [_VP]
+        lib.wbte_server_create.argtypes = [_I32, ctypes.c_uint32, ctypes.c_uint32, _U64, ctypes.POINTER(_VP)]
+        lib.wbte_submit.argtypes = [_VP, _VP, ctypes.POINTER(_U64)]
+        lib.wbte_poll.argtypes = [_VP, _U64, _U64, ctypes.POINTER(_I32)]
+        lib.wbte_server_destroy.argtypes = [_VP]
+        for name in ("wbte_crs_upload_wbtx", "wbte_crs_upload_wpfe", "wbte_crs_destroy", "wbte_server_create",
+                     "wbte_submit", "wbte_poll", "wbte_server_destroy"):
+            getattr(lib, name).restype = _I32
         # context-free, allocation-free G1 MSM: (out, points, scalars, n, stream)
         lib.wbte_g1_msm_static.argtypes = [_VP, _VP, _VP, _U64, _VP]
         lib.wbte_g1_msm_static.restype = _I32

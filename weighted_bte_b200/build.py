@@ -23,7 +23,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libwbte.so")
-SOURCES = ["k_arith.cu", "k_gt.cu", "k_hash.cu", "k_msm.cu", "k_opening.cu", "k_pairing.cu", "runtime.cu"]
+SOURCES = ["k_arith.cu", "k_gt.cu", "k_hash.cu", "k_msm.cu", "k_opening.cu", "k_pairing.cu", "runtime.cu", "server.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INCLUDE]
 # Code-layout variant of the shipped library (see fields.cuh): one out-of-line

@@ -509,14 +509,85 @@ __global__ void __launch_bounds__(WARP) k_small_msm(uint8_t* out, const uint8_t*
         store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * o), to_affine(load_vec(sh + lane)));
 }
 
+// XYZZ to affine for n points sharing one field inversion per chunk of C
+// consecutive points (Montgomery's trick): x = X / ZZ, y = Y / ZZZ with
+// 1 / (ZZ ZZZ) from the chunk's prefix products, which the forward pass
+// keeps in the x slots of the output.  The point at infinity (ZZ = 0)
+// skips the products and is written as zero bytes.
 template <class F>
-__global__ void k_xyzz_to_affine(uint8_t* out, const uint8_t* work, int64_t n) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void k_xyzz_to_affine_batch(uint8_t* out, const uint8_t* work, int64_t n, int64_t C) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t lo = t * C, hi = lo + C < n ? lo + C : n;
+    if (lo >= n) return;
     using A = Affine<F>;
-    Xyzz<F> p = load_vec(reinterpret_cast<const Xyzz<F>*>(work) + i);
-    store_affine(reinterpret_cast<A*>(out + GroupOf<F>::AFF * i), to_affine(p));
+    const Xyzz<F>* in = reinterpret_cast<const Xyzz<F>*>(work);
+    A* o = reinterpret_cast<A*>(out);
+    F acc;
+    f_set_one(acc);
+    for (int64_t i = lo; i < hi; i++) {
+        const Xyzz<F> p = load_vec(in + i);
+        A pre;
+        pre.x = acc;
+        f_set_zero(pre.y);
+        store_affine(o + i, pre);
+        if (!is_inf(p)) acc = f_mul(acc, f_mul(p.ZZ, p.ZZZ));
+    }
+    F inv = f_inv(acc);
+    for (int64_t i = hi - 1; i >= lo; i--) {
+        const Xyzz<F> p = load_vec(in + i);
+        A r;
+        if (is_inf(p)) {
+            set_inf(r);
+        } else {
+            const F w = f_mul(p.ZZ, p.ZZZ);
+            const F t_i = f_mul(inv, load_vec(o + i).x);  // 1 / (ZZ_i ZZZ_i), written above (plain load)
+            inv = f_mul(inv, w);
+            r.x = f_mul(p.X, f_mul(t_i, p.ZZZ));
+            r.y = f_mul(p.Y, f_mul(t_i, p.ZZ));
+        }
+        store_affine(o + i, r);
+    }
 }
+
+// blst's projective points (Jacobian X, Y, Z: x = X / Z^2, y = Y / Z^3) to
+// affine, one inversion per chunk of C points (blst_p{1,2}s_to_affine);
+// Z = 0 gives the all-zero identity.
+template <class F>
+__global__ void k_jacobian_to_affine_batch(uint8_t* out, const uint8_t* in, int64_t n, int64_t C) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t lo = t * C, hi = lo + C < n ? lo + C : n;
+    if (lo >= n) return;
+    using A = Affine<F>;
+    struct Jac { F X, Y, Z; };
+    const Jac* P = reinterpret_cast<const Jac*>(in);
+    A* o = reinterpret_cast<A*>(out);
+    F acc;
+    f_set_one(acc);
+    for (int64_t i = lo; i < hi; i++) {
+        const Jac p = load_vec(P + i);
+        A pre;
+        pre.x = acc;
+        f_set_zero(pre.y);
+        store_affine(o + i, pre);
+        if (!f_is_zero(p.Z)) acc = f_mul(acc, p.Z);
+    }
+    F inv = f_inv(acc);
+    for (int64_t i = hi - 1; i >= lo; i--) {
+        const Jac p = load_vec(P + i);
+        A r;
+        if (f_is_zero(p.Z)) {
+            set_inf(r);
+        } else {
+            const F zi = f_mul(inv, load_vec(o + i).x);  // 1 / Z_i, written above (plain load)
+            inv = f_mul(inv, p.Z);
+            const F z2 = f_sqr(zi);
+            r.x = f_mul(p.X, z2);
+            r.y = f_mul(p.Y, f_mul(z2, zi));
+        }
+        store_affine(o + i, r);
+    }
+}
+
 
 // ------------------------------------------------------------ encodings
 WBTE_INL void fp_store_be48(uint8_t* out, const Fp& m) {
@@ -936,6 +1007,34 @@ static bool ntt_joint(Group g, int64_t butterflies) {
     return joint < lane;
 }
 
+// Points per thread of the batched conversions: one inversion (about 485
+// Fp products) per chunk against about 7 products per point, so chunks grow
+// only while the launch still fills the resident threads.
+static int64_t normalize_chunk(int64_t n) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t resident = (int64_t)(sms > 0 ? sms : 148) * 256;
+    int64_t C = n / resident;
+    return C < 1 ? 1 : (C > 32 ? 32 : C);
+}
+
+void launch_xyzz_to_affine(Group g, uint8_t* out, const uint8_t* work, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    const int64_t C = normalize_chunk(n), threads = (n + C - 1) / C;
+    note_launch();
+    if (g == GROUP_G1) k_xyzz_to_affine_batch<Fp><<<blocks_for(threads), TPB, 0, s>>>(out, work, n, C);
+    else k_xyzz_to_affine_batch<Fp2><<<blocks_for(threads), TPB, 0, s>>>(out, work, n, C);
+}
+
+void launch_batch_normalize(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    const int64_t C = normalize_chunk(n), threads = (n + C - 1) / C;
+    note_launch();
+    if (g == GROUP_G1) k_jacobian_to_affine_batch<Fp><<<blocks_for(threads), TPB, 0, s>>>(out, in, n, C);
+    else k_jacobian_to_affine_batch<Fp2><<<blocks_for(threads), TPB, 0, s>>>(out, in, n, C);
+}
+
 void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, int64_t n, cudaStream_t s, int64_t count) {
     ProfScope prof_(g == GROUP_G1 ? "ntt_g1" : "ntt_g2", s);
     if (n <= 0 || count <= 0) return;
@@ -954,7 +1053,7 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
                 k_ntt_stage<Fp><<<blocks_for(NttLanes<Fp>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
         }
         note_launch();
-        k_xyzz_to_affine<Fp><<<blocks_for(total), TPB, 0, s>>>(io, work, total);
+        launch_xyzz_to_affine(GROUP_G1, io, work, total, s);
     } else {
         note_launch();
         k_ntt_load<Fp2><<<blocks_for(total), TPB, 0, s>>>(work, io, n, bits, count);
@@ -967,7 +1066,7 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
                 k_ntt_stage<Fp2><<<blocks_for(NttLanes<Fp2>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
         }
         note_launch();
-        k_xyzz_to_affine<Fp2><<<blocks_for(total), TPB, 0, s>>>(io, work, total);
+        launch_xyzz_to_affine(GROUP_G2, io, work, total, s);
     }
 }
 

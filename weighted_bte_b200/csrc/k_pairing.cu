@@ -2,6 +2,7 @@
 // exponentiation and the GT element kernels (products, masks, encodings).
 // The GT transforms live in k_gt.cu.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 
 #include "launch.h"
@@ -90,6 +91,52 @@ __global__ void WBTE_PAIR_BOUNDS k_final_exp(uint8_t* out, const uint8_t* in, in
         final_exp_hard(r, r);
     }
     store_vec(as_gt(out) + i, r);
+}
+
+WBTE_INL bool fp12_is_zero(const Fp12& a) {
+    const uint32_t* x = reinterpret_cast<const uint32_t*>(&a);
+    uint32_t d = 0;
+    for (int i = 0; i < 144; i++) d |= x[i];
+    return d == 0;
+}
+
+// The easy part f^((p^6 - 1)(p^2 + 1)) of C consecutive values per thread
+// sharing one Fp12 inversion (batch_easy_final_exponentiation,
+// btx/src/final_exponentiation.rs:228-252): the forward pass keeps the prefix
+// products in `pre`, one inversion of the chunk's product, and each value's
+// inverse falls out on the way back.  A zero value (no inverse) is left out
+// of the product and gives zero, as the per-value kernel does.  full: the
+// hard part follows.  in may equal out.
+__global__ void WBTE_PAIR_BOUNDS k_final_exp_easy_batch(uint8_t* out, const uint8_t* in, uint8_t* pre, int64_t n,
+                                                        int64_t C, int full) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t lo = t * C, hi = lo + C < n ? lo + C : n;
+    if (lo >= n) return;
+    Fp12 acc = fp12_one();
+    for (int64_t i = lo; i < hi; i++) {
+        const Fp12 f = load_vec(as_gt(in) + i);
+        store_vec(as_gt(pre) + i, acc);
+        if (!fp12_is_zero(f)) fp12_mul(acc, acc, f);
+    }
+    Fp12 inv;
+    fp12_inv(inv, acc);
+    for (int64_t i = hi - 1; i >= lo; i--) {
+        const Fp12 f = load_vec(as_gt(in) + i);
+        Fp12 r;
+        if (fp12_is_zero(f)) {
+            r = f;
+        } else {
+            Fp12 fi, u;
+            fp12_mul(fi, inv, load_vec(as_gt(pre) + i));  // 1 / f_i
+            fp12_mul(inv, inv, f);
+            fp12_conj(r, f);
+            fp12_mul(r, r, fi);  // f^(p^6 - 1)
+            fp12_frobenius(u, r, 2);
+            fp12_mul(r, r, u);  // ^(p^2 + 1)
+            if (full) final_exp_hard(r, r);
+        }
+        store_vec(as_gt(out) + i, r);
+    }
 }
 
 __global__ void k_fp12_mul(uint8_t* out, const uint8_t* a, int64_t sa, const uint8_t* b, int64_t sb, bool conj_b, int64_t n) {
@@ -198,9 +245,37 @@ void launch_fp12_segment_product(uint8_t* out, const uint8_t* in, const int64_t*
     note_launch();
     k_fp12_segment_product<<<blocks_for(k), TPB, 0, s>>>(out, in, offsets, k);
 }
+// Values per thread of the batched easy part: one Fp12 inversion (about 600
+// Fp products) per chunk against three products per value, so chunks grow
+// only while the launch still fills the resident threads.
+static int64_t easy_chunk(int64_t n) {
+    static std::atomic<int64_t> resident{0};
+    int64_t r = resident.load();
+    if (r == 0) {
+        int dev = 0, sms = 0, blocks = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_final_exp_easy_batch, TPB, 0);
+        r = (int64_t)(sms > 0 ? sms : 148) * (blocks > 0 ? blocks : 1) * TPB;
+        resident.store(r);
+    }
+    const int64_t C = n / r;
+    return C < 1 ? 1 : (C > 8 ? 8 : C);
+}
+
 void launch_final_exp(uint8_t* out, const uint8_t* in, int64_t n, FinalExpMode mode, cudaStream_t s) {
     ProfScope prof_(mode == FE_EASY ? "final_exp_easy" : (mode == FE_HARD ? "final_exp_hard" : "final_exp"), s);
     if (n <= 0) return;
+    const int64_t C = mode == FE_HARD ? 1 : easy_chunk(n);
+    uint8_t* pre = nullptr;
+    if (C > 1 && cudaMallocAsync(&pre, GT_SZ * (size_t)n, s) == cudaSuccess) {
+        const int64_t threads = (n + C - 1) / C;
+        note_launch();
+        k_final_exp_easy_batch<<<blocks_for(threads), TPB, 0, s>>>(out, in, pre, n, C, mode == FE_FULL ? 1 : 0);
+        cudaFreeAsync(pre, s);
+        return;
+    }
+    cudaGetLastError();
     note_launch();
     k_final_exp<<<blocks_for(n), TPB, 0, s>>>(out, in, n, (int)mode);
 }

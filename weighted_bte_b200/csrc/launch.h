@@ -78,6 +78,10 @@ void launch_mul_pow2(Group g, uint8_t* out, const uint8_t* in, int64_t n, int k,
 // out[j] = sum over t in [offsets[j], offsets[j+1]) of in[t] (affine in/out)
 void launch_segment_sum(Group g, uint8_t* out, const uint8_t* in, const int64_t* offsets, int64_t k, cudaStream_t s);
 void launch_negate(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
+// XYZZ points (work) to affine (out), one inversion per chunk (Montgomery's trick)
+void launch_xyzz_to_affine(Group g, uint8_t* out, const uint8_t* work, int64_t n, cudaStream_t s);
+// blst projective (Jacobian X, Y, Z) points to affine, one inversion per chunk
+void launch_batch_normalize(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
 // radix-2 DIT transform of n affine points in place (forward or unscaled inverse)
 void launch_group_ntt(Group g, uint8_t* io_affine, uint8_t* work_xyzz, const uint8_t* twiddles, int64_t n, cudaStream_t s,
                       int64_t count = 1);

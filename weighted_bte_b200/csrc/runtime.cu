@@ -246,6 +246,39 @@ void fp12_segments_product(Call& c, uint8_t* out, const uint8_t* in, int64_t len
     }
 }
 
+// out[j] = product of in[offs[j] .. offs[j+1]) for the k = offs.size() - 1
+// segments of any lengths, by levels of products of at most 16 consecutive
+// values inside each segment, so that long segments spread over many
+// threads (doffs: offs already on the device)
+void fp12_ragged_product(Call& c, uint8_t* out, const uint8_t* in, std::vector<int64_t> offs, const int64_t* doffs) {
+    const int64_t G = 16;
+    const size_t k = offs.size() - 1;
+    const uint8_t* cur = in;
+    while (true) {
+        int64_t longest = 0;
+        for (size_t j = 0; j < k; j++) longest = std::max(longest, offs[j + 1] - offs[j]);
+        if (longest <= G) {
+            launch_fp12_segment_product(out, cur, doffs, (int64_t)k, c.s);
+            return;
+        }
+        // groups of G inside every segment; segment j keeps its groups
+        std::vector<int64_t> goffs(1, 0), next(1, 0);
+        for (size_t j = 0; j < k; j++) {
+            for (int64_t x = offs[j]; x < offs[j + 1]; x += G) goffs.push_back(std::min(offs[j + 1], x + G));
+            next.push_back((int64_t)goffs.size() - 1);
+        }
+        const int64_t groups = (int64_t)goffs.size() - 1;
+        uint8_t* dst = c.alloc(GT_SZ * (size_t)std::max<int64_t>(groups, 1));
+        const int64_t* dg = c.in_vec(goffs);
+        const int64_t* dn = c.in_vec(next);
+        if (!c.ok()) return;
+        launch_fp12_segment_product(dst, cur, dg, groups, c.s);
+        cur = dst;
+        offs = next;
+        doffs = dn;
+    }
+}
+
 // G2 generator affine bytes on the device
 uint8_t* g2_generator_dev(Call& c) {
     uint8_t one[32] = {1};
@@ -572,6 +605,23 @@ int32_t wbte_g1_decompress(wbte_ctx* ctx, void* out, uint8_t* status, const void
 int32_t wbte_g2_decompress(wbte_ctx* ctx, void* out, uint8_t* status, const void* in, uint64_t n, int32_t check_group) {
     return decompress_impl(ctx, GROUP_G2, out, status, in, n, check_group);
 }
+static int32_t normalize_impl(wbte_ctx* ctx, Group g, void* out, const void* in, uint64_t n) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (n == 0) return c.finish();
+    if (!out || !in) return c.fail(WBTE_ERR_INVALID_ARG, "null argument");
+    const size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF;
+    uint8_t* d = c.out(out, aff * n);
+    const uint8_t* di = c.in(in, 3 * (aff / 2) * n);
+    if (c.ok()) launch_batch_normalize(g, d, di, (int64_t)n, c.s);
+    return c.finish();
+}
+int32_t wbte_g1_batch_normalize(wbte_ctx* ctx, void* out, const void* in, uint64_t n) {
+    return normalize_impl(ctx, GROUP_G1, out, in, n);
+}
+int32_t wbte_g2_batch_normalize(wbte_ctx* ctx, void* out, const void* in, uint64_t n) {
+    return normalize_impl(ctx, GROUP_G2, out, in, n);
+}
 int32_t wbte_g1_compress(wbte_ctx* ctx, void* out, const void* in, uint64_t n) { return compress_impl(ctx, GROUP_G1, out, in, n); }
 int32_t wbte_g2_compress(wbte_ctx* ctx, void* out, const void* in, uint64_t n) { return compress_impl(ctx, GROUP_G2, out, in, n); }
 
@@ -698,7 +748,7 @@ int32_t wbte_multi_miller_loop(wbte_ctx* ctx, void* out, const void* p, const vo
     const int64_t* doffs = c.in_vec(ho);
     if (!c.ok()) return c.finish();
     launch_miller(f, dp, dq, n, c.s);
-    launch_fp12_segment_product(d, f, doffs, (int64_t)k, c.s);
+    fp12_ragged_product(c, d, f, ho, doffs);
     return c.finish();
 }
 int32_t wbte_final_exp(wbte_ctx* ctx, void* out, const void* in, uint64_t n, int32_t mode) {
