@@ -124,7 +124,7 @@ def test_weighted_pfe_classes_through_the_abi_server():
     assert lib.wbte_server_create(0, 3, 8, 0, ctypes.byref(srv)) == WBTE_OK
     rng = ChaCha20Rng.seed_from_u64(62)
     pending = []
-    for k, s in enumerate([3, 8, 4, 6, 2, 7]):
+    for k, s in enumerate([3, 8, 4, 6, 3, 7]):
         B = wpb.size_class(s)
         sc = classes[B]
         msgs = gt_msgs(s, 11 * (k + 3))

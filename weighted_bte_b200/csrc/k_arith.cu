@@ -1007,6 +1007,29 @@ static bool ntt_joint(Group g, int64_t butterflies) {
     return joint < lane;
 }
 
+// work[i] = [c_i] in[i] for small signed c_i (XYZZ out): double-and-add over
+// the bits of |c_i| with mixed additions of the affine input, negated for
+// negative c_i -- mul_group_signed_small, weighted_pfe/src/decryption.rs:736-760.
+template <class F>
+__global__ void k_mul_small(uint8_t* work, const uint8_t* in, const int32_t* coeffs, int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    using A = Affine<F>;
+    const int32_t c = coeffs[i];
+    const uint32_t mag = c < 0 ? (uint32_t)(-(int64_t)c) : (uint32_t)c;
+    Xyzz<F> acc;
+    set_inf(acc);
+    if (mag) {
+        const A p = load_affine(reinterpret_cast<const A*>(in + GroupOf<F>::AFF * i));
+        for (int b = 31 - __clz(mag); b >= 0; b--) {
+            acc = xyzz_dbl(acc);
+            if ((mag >> b) & 1) acc = xyzz_madd(acc, p);
+        }
+        if (c < 0) acc = neg(acc);
+    }
+    store_vec(reinterpret_cast<Xyzz<F>*>(work) + i, acc);
+}
+
 // Points per thread of the batched conversions: one inversion (about 485
 // Fp products) per chunk against about 7 products per point, so chunks grow
 // only while the launch still fills the resident threads.
@@ -1027,6 +1050,17 @@ void launch_xyzz_to_affine(Group g, uint8_t* out, const uint8_t* work, int64_t n
     else k_xyzz_to_affine_batch<Fp2><<<blocks_for(threads), TPB, 0, s>>>(out, work, n, C);
 }
 
+void launch_mul_small(Group g, uint8_t* out, const uint8_t* in, const int32_t* coeffs, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    uint8_t* work = nullptr;
+    if (cudaMallocAsync(&work, (g == GROUP_G1 ? G1_XYZZ : G2_XYZZ) * (size_t)n, s) != cudaSuccess) return;
+    note_launch();
+    if (g == GROUP_G1) k_mul_small<Fp><<<blocks_for(n), TPB, 0, s>>>(work, in, coeffs, n);
+    else k_mul_small<Fp2><<<blocks_for(n), TPB, 0, s>>>(work, in, coeffs, n);
+    launch_xyzz_to_affine(g, out, work, n, s);
+    cudaFreeAsync(work, s);
+}
+
 void launch_batch_normalize(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s) {
     if (n <= 0) return;
     const int64_t C = normalize_chunk(n), threads = (n + C - 1) / C;
@@ -1036,8 +1070,16 @@ void launch_batch_normalize(Group g, uint8_t* out, const uint8_t* in, int64_t n,
 }
 
 void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, int64_t n, cudaStream_t s, int64_t count) {
-    ProfScope prof_(g == GROUP_G1 ? "ntt_g1" : "ntt_g2", s);
     if (n <= 0 || count <= 0) return;
+    if (g == GROUP_G1 && count > WARP && count % WARP != 0) {
+        // the largest multiple of 32 transforms takes the warp-uniform NAF
+        // twiddles of k_ntt_stage_joint; the rest runs on its own
+        const int64_t a = count - count % WARP;
+        launch_group_ntt(g, io, work, tw, n, s, a);
+        launch_group_ntt(g, io + G1_AFF * (size_t)(n * a), work + G1_XYZZ * (size_t)(n * a), tw, n, s, count - a);
+        return;
+    }
+    ProfScope prof_(g == GROUP_G1 ? "ntt_g1" : "ntt_g2", s);
     int bits = 0;
     while ((int64_t(1) << bits) < n) bits++;
     const int64_t total = n * count, butterflies = (n / 2) * count;

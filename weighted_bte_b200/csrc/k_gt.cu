@@ -324,7 +324,37 @@ __global__ void __launch_bounds__(WARP, WBTE_GT_MINBLOCKS) k_gt_pow(uint8_t* out
     if (active && c == 0) store_vec(as_gt(out) + i, load_vec(sh + lane));
 }
 
+// out[i] = base[i stride]^c_i for small signed c_i on cyclotomic values:
+// square-and-multiply over the bits of |c_i| with cyclotomic squarings, then
+// the inverse (conjugation) for negative c_i -- mul_cyclotomic_signed_small of
+// weighted_pfe/src/fft.rs:671-699.  c_i = 0 gives one.
+__global__ void k_gt_pow_small(uint8_t* out, const uint8_t* base, int64_t stride, const int32_t* coeffs, int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t c = coeffs[i];
+    uint32_t mag = c < 0 ? (uint32_t)(-(int64_t)c) : (uint32_t)c;
+    Fp12 acc = fp12_one();
+    if (mag) {
+        const Fp12 x = load_vec(as_gt(base) + stride * i);
+        acc = x;
+        for (int b = 30 - __clz(mag); b >= 0; b--) {
+            fp12_cyclotomic_sqr(acc, acc);
+            if ((mag >> b) & 1) fp12_mul(acc, acc, x);
+        }
+        if (c < 0) fp12_conj(acc, acc);
+    }
+    store_vec(as_gt(out) + i, acc);
+}
+
 }  // namespace
+
+void launch_gt_pow_small(uint8_t* out, const uint8_t* base, int64_t stride, const int32_t* coeffs, int64_t n,
+                         cudaStream_t s) {
+    ProfScope prof_("gt_pow_small", s);
+    if (n <= 0) return;
+    note_launch();
+    k_gt_pow_small<<<blocks_for(n), TPB, 0, s>>>(out, base, stride, coeffs, n);
+}
 
 // Lanes per exponentiation for a radix-4 stage of E twiddle powers, from a
 // cost model: one lane's work in Fp products (65 squarings and 74 products
@@ -361,8 +391,16 @@ static int gt_pow_lanes(int64_t E, bool shared_plan) {
 
 static void gt_transform(uint8_t* io, const uint8_t* tw, int64_t n, int64_t out_count, bool prefix, cudaStream_t s,
                          int64_t count, bool inverse) {
-    ProfScope prof_("gt_ifft", s);
     if (n <= 1 || count <= 0) return;
+    if (count > WARP && count % WARP != 0) {
+        // the largest multiple of 32 transforms takes the warp-uniform plan
+        // kernels; the rest runs on its own
+        const int64_t a = count - count % WARP;
+        gt_transform(io, tw, n, out_count, prefix, s, a, inverse);
+        gt_transform(io + GT_SZ * (size_t)(n * a), tw, n, out_count, prefix, s, count - a, inverse);
+        return;
+    }
+    ProfScope prof_("gt_ifft", s);
     int bits = 0;
     while ((int64_t(1) << bits) < n) bits++;
     uint8_t* tmp = nullptr;

@@ -80,6 +80,8 @@ void launch_segment_sum(Group g, uint8_t* out, const uint8_t* in, const int64_t*
 void launch_negate(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
 // XYZZ points (work) to affine (out), one inversion per chunk (Montgomery's trick)
 void launch_xyzz_to_affine(Group g, uint8_t* out, const uint8_t* work, int64_t n, cudaStream_t s);
+// out[i] = [c_i] in[i] for small signed integers c_i (affine in and out)
+void launch_mul_small(Group g, uint8_t* out, const uint8_t* in, const int32_t* coeffs, int64_t n, cudaStream_t s);
 // blst projective (Jacobian X, Y, Z) points to affine, one inversion per chunk
 void launch_batch_normalize(Group g, uint8_t* out, const uint8_t* in, int64_t n, cudaStream_t s);
 // radix-2 DIT transform of n affine points in place (forward or unscaled inverse)
@@ -156,6 +158,9 @@ void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* twiddles_inv, int
 void launch_gt_ntt(uint8_t* io, const uint8_t* twiddles, int64_t n, cudaStream_t s, int64_t count = 1, bool inverse = false);
 // out[i] = base[i * stride]^scalars[i] on GT
 void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t base_stride, const uint8_t* scalars, int64_t n, cudaStream_t s);
+// out[i] = base[i * stride]^coeffs[i] on cyclotomic values, small signed exponents
+void launch_gt_pow_small(uint8_t* out, const uint8_t* base, int64_t stride, const int32_t* coeffs, int64_t n,
+                         cudaStream_t s);
 // out[i] = a[i * sa] * b[i * sb] (conj_b: b conjugated)
 void launch_fp12_mul(uint8_t* out, const uint8_t* a, int64_t sa, const uint8_t* b, int64_t sb, bool conj_b, int64_t n, cudaStream_t s);
 // out[i] = conjugate of in[i] (the inverse in the cyclotomic subgroup)

@@ -1472,14 +1472,16 @@ int32_t wbte_wpfe_prepare(wbte_ctx* ctx, const wbte_wpfe_key* key, const int64_t
 static bool wpfe_precompute_core(Call& c, uint8_t* dfc, uint8_t* dpc, const uint8_t* dfirst, const uint8_t* dl,
                                  uint64_t B, uint64_t K) {
     const uint64_t n = B * K;
-    std::vector<int64_t> coeff(n);
-    std::vector<int32_t> rot(n);
+    std::vector<int32_t> coeff(n), rot(n);
     for (uint64_t b = 0; b < K; b++)
         for (uint64_t k = 0; k < B; k++) {
-            coeff[b * B + k] = (int64_t)B - 1 - 2 * (int64_t)k;
+            coeff[b * B + k] = (int32_t)B - 1 - 2 * (int32_t)k;
             rot[b * B + k] = (int32_t)(b * B + (k + B - 1) % B);
         }
-    const uint8_t* dcoef = c.in_vec(fr_small_signed(coeff));
+    // the spectrum's coefficients are small signed integers: double-and-add
+    // and square-and-multiply over their bits (mul_group_signed_small,
+    // mul_cyclotomic_signed_small), not full scalar multiplications
+    const int32_t* dcoef = c.in_vec(coeff);
     const int32_t* drot = c.in_vec(rot);
     uint8_t* x = c.alloc(G1_AFF * n);
     uint8_t* y = c.alloc(G1_AFF * n);
@@ -1492,7 +1494,7 @@ static bool wpfe_precompute_core(Call& c, uint8_t* dfc, uint8_t* dpc, const uint
     // G1: 2B sum_{k != i} first_k / (alpha_k - alpha_i) (:683-708)
     cudaMemcpyAsync(x, dfirst, G1_AFF * n, cudaMemcpyDeviceToDevice, c.s);
     if (B > 1) launch_group_ntt(GROUP_G1, x, work, tw, (int64_t)B, c.s, (int64_t)K);
-    launch_mul_batch(GROUP_G1, y, x, 1, dcoef, (int64_t)n, c.s);
+    launch_mul_small(GROUP_G1, y, x, dcoef, (int64_t)n, c.s);
     launch_gather(x, y, drot, (int64_t)n, G1_AFF, c.s);
     launch_negate(GROUP_G1, x, x, (int64_t)n, c.s);
     if (B > 1) launch_group_ntt(GROUP_G1, x, work, twi, (int64_t)B, c.s, (int64_t)K);
@@ -1501,7 +1503,7 @@ static bool wpfe_precompute_core(Call& c, uint8_t* dfc, uint8_t* dpc, const uint
     launch_miller_lines(f, dl, dfirst, (int64_t)n, c.s, (int64_t)B);
     launch_final_exp(f, f, (int64_t)n, FE_EASY, c.s);
     if (B > 1) launch_gt_ntt(f, tw, (int64_t)B, c.s, (int64_t)K);
-    launch_gt_pow(h, f, 1, dcoef, (int64_t)n, c.s);
+    launch_gt_pow_small(h, f, 1, dcoef, (int64_t)n, c.s);
     launch_gather(f, h, drot, (int64_t)n, GT_SZ, c.s);
     launch_fp12_conj(f, f, (int64_t)n, c.s);
     if (B > 1) launch_gt_ntt(f, twi, (int64_t)B, c.s, (int64_t)K, true);
