@@ -386,6 +386,24 @@ int32_t wbte_btx_verify(wbte_ctx *ctx, int32_t *ok, const void *first, const uin
 int32_t wbte_btx_open(wbte_ctx *ctx, void *messages, const void *opening_lines, const void *sigma,
                       const void *second, const void *beta, const uint8_t *valid, uint64_t batch_size);
 
+/* The batched form of btx: K batches of one size B against one key
+ * (batch-major arrays), each kernel launched once over all K batches; per
+ * batch the results equal the single-batch calls':
+ *   precompute_many  beta K*B GT over the m kernel line tables (as wbte_btx_precompute)
+ *   open_many        messages K*B GT; opening_lines B tables; sigma K G1 (one
+ *                    combined share per batch); second, beta K*B GT; valid K*B
+ *   decrypt_many     precompute_many then open_many in one call, the cross
+ *                    terms and the opening pairing meeting before one hard part
+ *                    per slot (btx/src/decryption.rs:201-246, :402-458). */
+int32_t wbte_btx_precompute_many(wbte_ctx *ctx, void *beta, const void *kernel_lines, const void *first,
+                                 const uint8_t *valid, uint64_t batch_size, uint64_t K);
+int32_t wbte_btx_open_many(wbte_ctx *ctx, void *messages, const void *opening_lines, const void *sigma,
+                           const void *second, const void *beta, const uint8_t *valid, uint64_t batch_size,
+                           uint64_t K);
+int32_t wbte_btx_decrypt_many(wbte_ctx *ctx, void *messages, const void *kernel_lines, const void *opening_lines,
+                              const void *first, const void *second, const uint8_t *valid, const void *sigma,
+                              uint64_t batch_size, uint64_t K);
+
 /* ---------------------------------------------------- weighted_pfe */
 typedef struct {
     const void *domain_points;     /* total_weight Fr: the virtual points             */
@@ -486,6 +504,22 @@ int32_t wbte_wpfe_decrypt_many(wbte_ctx *ctx, void *messages, const void *sigmas
                                const void *by_party_lines, const void *total_lines, const void *mask_lines,
                                const void *first, const void *second, const void *alpha_products, uint64_t B,
                                uint64_t K);
+
+/* The batched form of pfe: K batches of one size B against one kernel
+ * (batch-major arrays), per batch equal to the single-batch calls:
+ *   precompute_many  weighted_first K*B G1, weighted_pairings K*B GT from
+ *                    first K*B G1, the B key line tables and the 2 B scalars
+ *                    of wbte_pfe_precompute (shared by the batches)
+ *   open_many        messages K*B GT from first, second K*B G1, third K*B GT,
+ *                    weighted_first/pairings K*B, pre_decryption_key K G1 (one
+ *                    combined key per batch), neg_scaled_s1 B Fr and the B
+ *                    line tables of each kind (pfe/src/decryption.rs:417-469). */
+int32_t wbte_pfe_precompute_many(wbte_ctx *ctx, void *weighted_first, void *weighted_pairings, const void *first,
+                                 const void *key_lines, const void *scalars, uint64_t B, uint64_t K);
+int32_t wbte_pfe_open_many(wbte_ctx *ctx, void *messages, const void *first, const void *second, const void *third,
+                           const void *weighted_first, const void *weighted_pairings, const void *pre_decryption_key,
+                           const void *neg_scaled_s1, const void *key_lines, const void *generator_lines,
+                           const void *mix_lines, uint64_t B, uint64_t K);
 
 /* ---------------------------------------- resident keys and served form */
 /* A request loop in the library for callers without their own scheduler:

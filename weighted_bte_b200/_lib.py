@@ -175,6 +175,11 @@ _SIGNATURES = {
     "wbte_wpfe_precompute_many": [_VP, _VP, _VP, _VP, _U64, _U64],
     "wbte_wpfe_open_many": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64],
     "wbte_wpfe_decrypt_many": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64],
+    "wbte_btx_precompute_many": [_VP, _VP, _VP, _VP, _U64, _U64],
+    "wbte_btx_open_many": [_VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64],
+    "wbte_btx_decrypt_many": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64],
+    "wbte_pfe_precompute_many": [_VP, _VP, _VP, _VP, _VP, _U64, _U64],
+    "wbte_pfe_open_many": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64, _U64],
     "wbte_pfe_kernel": [_VP, _VP, _U64, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
     "wbte_pfe_precompute": [_VP, _VP, _VP, _VP, _VP, _U64],
     "wbte_pfe_open": [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _U64],

@@ -1229,26 +1229,87 @@ int32_t wbte_btx_verify(wbte_ctx* ctx, int32_t* ok, const void* first, const uin
 
 int32_t wbte_btx_open(wbte_ctx* ctx, void* messages, const void* opening_lines, const void* sigma, const void* second,
                       const void* beta, const uint8_t* valid, uint64_t B) {
+    return wbte_btx_open_many(ctx, messages, opening_lines, sigma, second, beta, valid, B, 1);
+}
+
+// P[b B + i] = sigma[b]: each slot's G1 point of the opening pairing
+// e(sigma_b, h_{-(i+1)}) (btx/src/decryption.rs:402-458)
+static const uint8_t* btx_opening_points(Call& c, const uint8_t* dsig, uint64_t B, uint64_t K) {
+    std::vector<int32_t> idx(B * K);
+    for (uint64_t o = 0; o < B * K; o++) idx[o] = (int32_t)(o / B);
+    const int32_t* di = c.in_vec(idx);
+    uint8_t* P = c.alloc(G1_AFF * B * K);
+    if (c.ok()) launch_gather(P, dsig, di, (int64_t)(B * K), G1_AFF, c.s);
+    return P;
+}
+
+int32_t wbte_btx_open_many(wbte_ctx* ctx, void* messages, const void* opening_lines, const void* sigma,
+                           const void* second, const void* beta, const uint8_t* valid, uint64_t B, uint64_t K) {
     if (!ctx) return WBTE_ERR_INVALID_ARG;
     Call c(ctx);
-    if (!messages || !opening_lines || !sigma || !second || !beta || !valid || B == 0)
+    if (!messages || !opening_lines || !sigma || !second || !beta || !valid || B == 0 || K == 0)
         return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
-    uint8_t* dm = c.out(messages, GT_SZ * B);
+    const uint64_t n = B * K;
+    uint8_t* dm = c.out(messages, GT_SZ * n);
     const uint8_t* dl = c.in(opening_lines, LINE_SZ * LINES_PER_POINT * B);
-    const uint8_t* dsig = c.in(sigma, G1_AFF);
-    const uint8_t* d2 = c.in(second, GT_SZ * B);
-    const uint8_t* db = c.in(beta, GT_SZ * B);
-    const uint8_t* dv = c.in(valid, B);
-    uint8_t* P = c.alloc(G1_AFF * B);
-    uint8_t* alpha = c.alloc(GT_SZ * B);
-    std::vector<int32_t> zero_idx(B, 0);
-    const int32_t* dz = c.in_vec(zero_idx);
+    const uint8_t* dsig = c.in(sigma, G1_AFF * K);
+    const uint8_t* d2 = c.in(second, GT_SZ * n);
+    const uint8_t* db = c.in(beta, GT_SZ * n);
+    const uint8_t* dv = c.in(valid, n);
+    uint8_t* alpha = c.alloc(GT_SZ * n);
+    const uint8_t* P = btx_opening_points(c, dsig, B, K);
     if (!c.ok()) return c.finish();
-    // alpha_slot = e(sigma, h_{-(slot+1)}) (btx/src/decryption.rs:402-458)
-    launch_gather(P, dsig, dz, (int64_t)B, G1_AFF, c.s);
-    launch_miller_lines(alpha, dl, P, (int64_t)B, c.s);
-    launch_final_exp(alpha, alpha, (int64_t)B, FE_FULL, c.s);
-    launch_unmask(dm, d2, alpha, db, dv, (int64_t)B, c.s);
+    launch_miller_lines(alpha, dl, P, (int64_t)n, c.s, (int64_t)B);
+    launch_final_exp(alpha, alpha, (int64_t)n, FE_FULL, c.s);
+    launch_unmask(dm, d2, alpha, db, dv, (int64_t)n, c.s);
+    return c.finish();
+}
+
+int32_t wbte_btx_precompute_many(wbte_ctx* ctx, void* beta, const void* kernel_lines, const void* first,
+                                 const uint8_t* valid, uint64_t B, uint64_t K) {
+    // the same middle product as weighted_btx's (btx/src/decryption.rs:201-246)
+    return wbte_wbtx_precompute_many(ctx, beta, kernel_lines, first, valid, B, K);
+}
+
+int32_t wbte_btx_decrypt_many(wbte_ctx* ctx, void* messages, const void* kernel_lines, const void* opening_lines,
+                              const void* first, const void* second, const uint8_t* valid, const void* sigma,
+                              uint64_t B, uint64_t K) {
+    if (!ctx) return WBTE_ERR_INVALID_ARG;
+    Call c(ctx);
+    if (!messages || !kernel_lines || !opening_lines || !first || !second || !valid || !sigma || B == 0 || K == 0)
+        return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
+    const uint64_t m = next_pow2(2 * B), n = B * K;
+    uint8_t* dm = c.out(messages, GT_SZ * n);
+    const uint8_t* dl = c.in(kernel_lines, LINE_SZ * LINES_PER_POINT * m);
+    const uint8_t* dol = c.in(opening_lines, LINE_SZ * LINES_PER_POINT * B);
+    const uint8_t* dfirst = c.in(first, G1_AFF * n);
+    const uint8_t* d2 = c.in(second, GT_SZ * n);
+    const uint8_t* dv = c.in(valid, n);
+    const uint8_t* dsig = c.in(sigma, G1_AFF * K);
+    uint8_t* x = c.zeros(G1_AFF * m * K);
+    uint8_t* work = c.alloc(G1_XYZZ * m * K);
+    uint8_t* f = c.alloc(GT_SZ * m * K);
+    uint8_t* y = c.alloc(GT_SZ * n);
+    uint8_t* alpha = c.alloc(GT_SZ * n);
+    const uint8_t* tw = twiddles(c, (int64_t)m, false);
+    const uint8_t* twi = twiddles(c, (int64_t)m, true);
+    const uint8_t* P = btx_opening_points(c, dsig, B, K);
+    if (!c.ok()) return c.finish();
+    // cross terms up to the truncated cyclotomic transform, the opening
+    // pairings up to their easy part, then one hard part per slot for
+    // beta / alpha (the hard part is a homomorphism of the cyclotomic subgroup)
+    cudaMemcpy2DAsync(x, G1_AFF * m, dfirst, G1_AFF * B, G1_AFF * B, K, cudaMemcpyDeviceToDevice, c.s);
+    launch_group_ntt(GROUP_G1, x, work, tw, (int64_t)m, c.s, (int64_t)K);
+    launch_miller_lines(f, dl, x, (int64_t)(m * K), c.s, (int64_t)m);
+    launch_final_exp(f, f, (int64_t)(m * K), FE_EASY, c.s);
+    launch_cyclotomic_prefix_ifft(f, twi, (int64_t)m, (int64_t)B, c.s, (int64_t)K);
+    launch_miller_lines(alpha, dol, P, (int64_t)n, c.s, (int64_t)B);
+    launch_final_exp(alpha, alpha, (int64_t)n, FE_EASY, c.s);
+    cudaMemcpy2DAsync(y, GT_SZ * B, f, GT_SZ * m, GT_SZ * B, K, cudaMemcpyDeviceToDevice, c.s);
+    launch_fp12_mul(y, y, 1, alpha, 1, true, (int64_t)n, c.s);
+    launch_final_exp(y, y, (int64_t)n, FE_HARD, c.s);
+    launch_fp12_mul(dm, d2, 1, y, 1, false, (int64_t)n, c.s);
+    launch_fp12_mask(dm, dv, (int64_t)n, c.s);
     return c.finish();
 }
 
@@ -1734,43 +1795,53 @@ int32_t wbte_wpfe_decrypt_many(wbte_ctx* ctx, void* messages, const void* sigmas
 // spec = NTT(io) * E.  E and cvec hold B Fr each (E[k] = B - 1 - 2k mod r,
 // cvec = B copies of c).  Group elements in affine form; GT in Fp12.
 static void pfe_conv_group(Call& c, Group g, uint8_t* io, const uint8_t* E, const uint8_t* cvec, const int32_t* rot,
-                           const int64_t* offs2, uint64_t B, const uint8_t* tw, const uint8_t* twi) {
+                           const int64_t* offs2, uint64_t B, const uint8_t* tw, const uint8_t* twi, uint64_t K = 1) {
+    // K transforms of B elements back to back; E, cvec, rot and offs2 cover all K B
     const size_t aff = g == GROUP_G1 ? G1_AFF : G2_AFF, xz = g == GROUP_G1 ? G1_XYZZ : G2_XYZZ;
-    uint8_t* work = c.alloc(xz * B);
-    uint8_t* a = c.alloc(aff * B);
-    uint8_t* b = c.alloc(aff * B);
-    uint8_t* pairs = c.alloc(2 * aff * B);
+    const uint64_t n = B * K;
+    uint8_t* work = c.alloc(xz * n);
+    uint8_t* a = c.alloc(aff * n);
+    uint8_t* b = c.alloc(aff * n);
+    uint8_t* pairs = c.alloc(2 * aff * n);
     if (!c.ok()) return;
-    if (B > 1) launch_group_ntt(g, io, work, tw, (int64_t)B, c.s);
-    launch_mul_batch(g, a, io, 1, E, (int64_t)B, c.s);
-    launch_gather(b, a, rot, (int64_t)B, aff, c.s);
-    launch_mul_batch(g, b, b, 1, cvec, (int64_t)B, c.s);
-    launch_negate(g, a, a, (int64_t)B, c.s);
-    cudaMemcpy2DAsync(pairs, 2 * aff, b, aff, aff, B, cudaMemcpyDeviceToDevice, c.s);
-    cudaMemcpy2DAsync(pairs + aff, 2 * aff, a, aff, aff, B, cudaMemcpyDeviceToDevice, c.s);
-    launch_segment_sum(g, io, pairs, offs2, (int64_t)B, c.s);
-    if (B > 1) launch_group_ntt(g, io, work, twi, (int64_t)B, c.s);
+    if (B > 1) launch_group_ntt(g, io, work, tw, (int64_t)B, c.s, (int64_t)K);
+    launch_mul_batch(g, a, io, 1, E, (int64_t)n, c.s);
+    launch_gather(b, a, rot, (int64_t)n, aff, c.s);
+    launch_mul_batch(g, b, b, 1, cvec, (int64_t)n, c.s);
+    launch_negate(g, a, a, (int64_t)n, c.s);
+    cudaMemcpy2DAsync(pairs, 2 * aff, b, aff, aff, n, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(pairs + aff, 2 * aff, a, aff, aff, n, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(g, io, pairs, offs2, (int64_t)n, c.s);
+    if (B > 1) launch_group_ntt(g, io, work, twi, (int64_t)B, c.s, (int64_t)K);
 }
 static void pfe_conv_gt(Call& c, uint8_t* io, const uint8_t* E, const uint8_t* cvec, const int32_t* rot, uint64_t B,
-                        const uint8_t* tw, const uint8_t* twi) {
-    uint8_t* a = c.alloc(GT_SZ * B);
-    uint8_t* b = c.alloc(GT_SZ * B);
-    uint8_t* h = c.alloc(GT_SZ * B);
+                        const uint8_t* tw, const uint8_t* twi, uint64_t K = 1) {
+    const uint64_t n = B * K;
+    uint8_t* a = c.alloc(GT_SZ * n);
+    uint8_t* b = c.alloc(GT_SZ * n);
+    uint8_t* h = c.alloc(GT_SZ * n);
     if (!c.ok()) return;
-    if (B > 1) launch_gt_ntt(io, tw, (int64_t)B, c.s);
-    launch_gt_pow(a, io, 1, E, (int64_t)B, c.s);
-    launch_gather(h, a, rot, (int64_t)B, GT_SZ, c.s);
-    launch_gt_pow(b, h, 1, cvec, (int64_t)B, c.s);
-    launch_fp12_mul(io, b, 1, a, 1, true, (int64_t)B, c.s);
-    if (B > 1) launch_gt_ntt(io, twi, (int64_t)B, c.s, 1, true);
+    if (B > 1) launch_gt_ntt(io, tw, (int64_t)B, c.s, (int64_t)K);
+    launch_gt_pow(a, io, 1, E, (int64_t)n, c.s);
+    launch_gather(h, a, rot, (int64_t)n, GT_SZ, c.s);
+    launch_gt_pow(b, h, 1, cvec, (int64_t)n, c.s);
+    launch_fp12_mul(io, b, 1, a, 1, true, (int64_t)n, c.s);
+    if (B > 1) launch_gt_ntt(io, twi, (int64_t)B, c.s, (int64_t)K, true);
 }
 
+// index tables of the convolution over K batches of B: rot[b B + i] = b B +
+// (i + 1) mod B, slot[b B + i] = i, batch[b B + i] = b, offs2 = 0, 2, 4, ..
 struct PfeConvTables {
-    std::vector<int32_t> rot;
+    std::vector<int32_t> rot, slot, batch;
     std::vector<int64_t> offs2;
-    explicit PfeConvTables(uint64_t B) : rot(B), offs2(B + 1) {
-        for (uint64_t i = 0; i < B; i++) rot[i] = (int32_t)((i + 1) % B);
-        for (uint64_t i = 0; i <= B; i++) offs2[i] = (int64_t)(2 * i);
+    explicit PfeConvTables(uint64_t B, uint64_t K = 1) : rot(B * K), slot(B * K), batch(B * K), offs2(B * K + 1) {
+        for (uint64_t b = 0; b < K; b++)
+            for (uint64_t i = 0; i < B; i++) {
+                rot[b * B + i] = (int32_t)(b * B + (i + 1) % B);
+                slot[b * B + i] = (int32_t)i;
+                batch[b * B + i] = (int32_t)b;
+            }
+        for (uint64_t i = 0; i <= B * K; i++) offs2[i] = (int64_t)(2 * i);
     }
 };
 
@@ -1833,33 +1904,44 @@ int32_t wbte_pfe_kernel(wbte_ctx* ctx, const void* fraction_keys, const void* ke
 
 int32_t wbte_pfe_precompute(wbte_ctx* ctx, void* weighted_first, void* weighted_pairings, const void* first,
                             const void* key_lines, const void* scalars, uint64_t B) {
+    return wbte_pfe_precompute_many(ctx, weighted_first, weighted_pairings, first, key_lines, scalars, B, 1);
+}
+
+int32_t wbte_pfe_precompute_many(wbte_ctx* ctx, void* weighted_first, void* weighted_pairings, const void* first,
+                                 const void* key_lines, const void* scalars, uint64_t B, uint64_t K) {
     if (!ctx) return WBTE_ERR_INVALID_ARG;
     Call c(ctx);
-    if (!weighted_first || !weighted_pairings || !first || !key_lines || !scalars || B == 0)
+    if (!weighted_first || !weighted_pairings || !first || !key_lines || !scalars || B == 0 || K == 0)
         return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
     if (log2_exact(B) < 0) return c.fail(WBTE_ERR_SIZE, "batch size must be a power of two");
-    uint8_t* dwf = c.out(weighted_first, G1_AFF * B);
-    uint8_t* dwp = c.out(weighted_pairings, GT_SZ * B);
-    const uint8_t* dfirst = c.in(first, G1_AFF * B);
+    const uint64_t n = B * K;
+    uint8_t* dwf = c.out(weighted_first, G1_AFF * n);
+    uint8_t* dwp = c.out(weighted_pairings, GT_SZ * n);
+    const uint8_t* dfirst = c.in(first, G1_AFF * n);
     const uint8_t* dkl = c.in(key_lines, LINE_SZ * LINES_PER_POINT * B);
     const uint8_t* sc = c.in(scalars, 2 * FR_SZ * B);
-    PfeConvTables tab(B);
+    PfeConvTables tab(B, K);
     const int32_t* drot = c.in_vec(tab.rot);
+    const int32_t* dslot = c.in_vec(tab.slot);
     const int64_t* doff2 = c.in_vec(tab.offs2);
-    uint8_t* x = c.alloc(G1_AFF * B);
-    uint8_t* f = c.alloc(GT_SZ * B);
+    uint8_t* x = c.alloc(G1_AFF * n);
+    uint8_t* f = c.alloc(GT_SZ * n);
+    uint8_t* E = c.alloc(FR_SZ * n);
+    uint8_t* cvec = c.alloc(FR_SZ * n);
     const uint8_t* tw = B > 1 ? twiddles(c, (int64_t)B, false) : nullptr;
     const uint8_t* twi = B > 1 ? twiddles(c, (int64_t)B, true) : nullptr;
     if (!c.ok()) return c.finish();
-    const uint8_t *E = sc, *cvec = sc + FR_SZ * B;
+    // the B scalars of each kind, repeated for every batch
+    launch_gather(E, sc, dslot, (int64_t)n, FR_SZ, c.s);
+    launch_gather(cvec, sc + FR_SZ * B, dslot, (int64_t)n, FR_SZ, c.s);
     // weighted convolution of the first components and of e(first_i, DK_i/(2B)) (pfe/src/decryption.rs:259-298)
-    cudaMemcpyAsync(x, dfirst, G1_AFF * B, cudaMemcpyDeviceToDevice, c.s);
-    pfe_conv_group(c, GROUP_G1, x, E, cvec, drot, doff2, B, tw, twi);
-    launch_miller_lines(f, dkl, dfirst, (int64_t)B, c.s);
-    launch_final_exp(f, f, (int64_t)B, FE_FULL, c.s);
-    pfe_conv_gt(c, f, E, cvec, drot, B, tw, twi);
-    cudaMemcpyAsync(dwf, x, G1_AFF * B, cudaMemcpyDeviceToDevice, c.s);
-    cudaMemcpyAsync(dwp, f, GT_SZ * B, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpyAsync(x, dfirst, G1_AFF * n, cudaMemcpyDeviceToDevice, c.s);
+    pfe_conv_group(c, GROUP_G1, x, E, cvec, drot, doff2, B, tw, twi, K);
+    launch_miller_lines(f, dkl, dfirst, (int64_t)n, c.s, (int64_t)B);
+    launch_final_exp(f, f, (int64_t)n, FE_FULL, c.s);
+    pfe_conv_gt(c, f, E, cvec, drot, B, tw, twi, K);
+    cudaMemcpyAsync(dwf, x, G1_AFF * n, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpyAsync(dwp, f, GT_SZ * n, cudaMemcpyDeviceToDevice, c.s);
     return c.finish();
 }
 
@@ -1867,54 +1949,65 @@ int32_t wbte_pfe_open(wbte_ctx* ctx, void* messages, const void* first, const vo
                       const void* weighted_first, const void* weighted_pairings, const void* pre_decryption_key,
                       const void* neg_scaled_s1, const void* key_lines, const void* generator_lines,
                       const void* mix_lines, uint64_t B) {
+    return wbte_pfe_open_many(ctx, messages, first, second, third, weighted_first, weighted_pairings,
+                              pre_decryption_key, neg_scaled_s1, key_lines, generator_lines, mix_lines, B, 1);
+}
+
+int32_t wbte_pfe_open_many(wbte_ctx* ctx, void* messages, const void* first, const void* second, const void* third,
+                           const void* weighted_first, const void* weighted_pairings, const void* pre_decryption_key,
+                           const void* neg_scaled_s1, const void* key_lines, const void* generator_lines,
+                           const void* mix_lines, uint64_t B, uint64_t K) {
     if (!ctx) return WBTE_ERR_INVALID_ARG;
     Call c(ctx);
     if (!messages || !first || !second || !third || !weighted_first || !weighted_pairings || !pre_decryption_key ||
-        !neg_scaled_s1 || !key_lines || !generator_lines || !mix_lines || B == 0)
+        !neg_scaled_s1 || !key_lines || !generator_lines || !mix_lines || B == 0 || K == 0)
         return c.fail(WBTE_ERR_INVALID_ARG, "null argument or empty batch");
     const size_t LT = LINE_SZ * LINES_PER_POINT * B;
-    uint8_t* dm = c.out(messages, GT_SZ * B);
-    const uint8_t* d1 = c.in(first, G1_AFF * B);
-    const uint8_t* d2 = c.in(second, G1_AFF * B);
-    const uint8_t* d3 = c.in(third, GT_SZ * B);
-    const uint8_t* dwf = c.in(weighted_first, G1_AFF * B);
-    const uint8_t* dwp = c.in(weighted_pairings, GT_SZ * B);
-    const uint8_t* dpdk = c.in(pre_decryption_key, G1_AFF);
+    const uint64_t n = B * K;
+    uint8_t* dm = c.out(messages, GT_SZ * n);
+    const uint8_t* d1 = c.in(first, G1_AFF * n);
+    const uint8_t* d2 = c.in(second, G1_AFF * n);
+    const uint8_t* d3 = c.in(third, GT_SZ * n);
+    const uint8_t* dwf = c.in(weighted_first, G1_AFF * n);
+    const uint8_t* dwp = c.in(weighted_pairings, GT_SZ * n);
+    const uint8_t* dpdk = c.in(pre_decryption_key, G1_AFF * K);
     const uint8_t* ds1 = c.in(neg_scaled_s1, FR_SZ * B);
     const uint8_t* dkl = c.in(key_lines, LT);
     const uint8_t* dgl = c.in(generator_lines, LT);
     const uint8_t* dml = c.in(mix_lines, LT);
-    PfeConvTables tab(B);
+    PfeConvTables tab(B, K);
     const int64_t* doff2 = c.in_vec(tab.offs2);
-    std::vector<int32_t> zero(B, 0);
-    const int32_t* dz = c.in_vec(zero);
-    uint8_t* npdk = c.alloc(G1_AFF * B);
-    uint8_t* pairs = c.alloc(2 * G1_AFF * B);
-    uint8_t* d = c.alloc(G1_AFF * B);
-    uint8_t* b1 = c.alloc(G1_AFF * B);
-    uint8_t* f0 = c.alloc(GT_SZ * B);
-    uint8_t* f1 = c.alloc(GT_SZ * B);
-    uint8_t* f2 = c.alloc(GT_SZ * B);
+    const int32_t* dslot = c.in_vec(tab.slot);
+    const int32_t* dbatch = c.in_vec(tab.batch);
+    uint8_t* npdk = c.alloc(G1_AFF * n);
+    uint8_t* s1 = c.alloc(FR_SZ * n);
+    uint8_t* pairs = c.alloc(2 * G1_AFF * n);
+    uint8_t* d = c.alloc(G1_AFF * n);
+    uint8_t* b1 = c.alloc(G1_AFF * n);
+    uint8_t* f0 = c.alloc(GT_SZ * n);
+    uint8_t* f1 = c.alloc(GT_SZ * n);
+    uint8_t* f2 = c.alloc(GT_SZ * n);
     if (!c.ok()) return c.finish();
-    // b1_i = weighted_first_i - 2B s1_i (second_i - pdk) (pfe/src/decryption.rs:434-447)
-    launch_gather(npdk, dpdk, dz, (int64_t)B, G1_AFF, c.s);
-    launch_negate(GROUP_G1, npdk, npdk, (int64_t)B, c.s);
-    cudaMemcpy2DAsync(pairs, 2 * G1_AFF, d2, G1_AFF, G1_AFF, B, cudaMemcpyDeviceToDevice, c.s);
-    cudaMemcpy2DAsync(pairs + G1_AFF, 2 * G1_AFF, npdk, G1_AFF, G1_AFF, B, cudaMemcpyDeviceToDevice, c.s);
-    launch_segment_sum(GROUP_G1, d, pairs, doff2, (int64_t)B, c.s);
-    launch_mul_batch(GROUP_G1, d, d, 1, ds1, (int64_t)B, c.s);
-    cudaMemcpy2DAsync(pairs, 2 * G1_AFF, dwf, G1_AFF, G1_AFF, B, cudaMemcpyDeviceToDevice, c.s);
-    cudaMemcpy2DAsync(pairs + G1_AFF, 2 * G1_AFF, d, G1_AFF, G1_AFF, B, cudaMemcpyDeviceToDevice, c.s);
-    launch_segment_sum(GROUP_G1, b1, pairs, doff2, (int64_t)B, c.s);
+    // b1_i = weighted_first_i - 2B s1_i (second_i - pdk) (pfe/src/decryption.rs:434-447), pdk of the slot's batch
+    launch_gather(npdk, dpdk, dbatch, (int64_t)n, G1_AFF, c.s);
+    launch_negate(GROUP_G1, npdk, npdk, (int64_t)n, c.s);
+    launch_gather(s1, ds1, dslot, (int64_t)n, FR_SZ, c.s);
+    cudaMemcpy2DAsync(pairs, 2 * G1_AFF, d2, G1_AFF, G1_AFF, n, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(pairs + G1_AFF, 2 * G1_AFF, npdk, G1_AFF, G1_AFF, n, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(GROUP_G1, d, pairs, doff2, (int64_t)n, c.s);
+    launch_mul_batch(GROUP_G1, d, d, 1, s1, (int64_t)n, c.s);
+    cudaMemcpy2DAsync(pairs, 2 * G1_AFF, dwf, G1_AFF, G1_AFF, n, cudaMemcpyDeviceToDevice, c.s);
+    cudaMemcpy2DAsync(pairs + G1_AFF, 2 * G1_AFF, d, G1_AFF, G1_AFF, n, cudaMemcpyDeviceToDevice, c.s);
+    launch_segment_sum(GROUP_G1, b1, pairs, doff2, (int64_t)n, c.s);
     // mask_i = e(second_i, [s2]) e(b1_i, DK_i/(2B)) e(first_i, mix_i) / weighted_pairings_i (:449-465)
-    launch_miller_lines(f0, dgl, d2, (int64_t)B, c.s);
-    launch_miller_lines(f1, dkl, b1, (int64_t)B, c.s);
-    launch_miller_lines(f2, dml, d1, (int64_t)B, c.s);
-    launch_fp12_mul(f0, f0, 1, f1, 1, false, (int64_t)B, c.s);
-    launch_fp12_mul(f0, f0, 1, f2, 1, false, (int64_t)B, c.s);
-    launch_final_exp(f0, f0, (int64_t)B, FE_FULL, c.s);
-    launch_fp12_mul(f0, f0, 1, dwp, 1, true, (int64_t)B, c.s);
-    launch_fp12_mul(dm, d3, 1, f0, 1, true, (int64_t)B, c.s);
+    launch_miller_lines(f0, dgl, d2, (int64_t)n, c.s, (int64_t)B);
+    launch_miller_lines(f1, dkl, b1, (int64_t)n, c.s, (int64_t)B);
+    launch_miller_lines(f2, dml, d1, (int64_t)n, c.s, (int64_t)B);
+    launch_fp12_mul(f0, f0, 1, f1, 1, false, (int64_t)n, c.s);
+    launch_fp12_mul(f0, f0, 1, f2, 1, false, (int64_t)n, c.s);
+    launch_final_exp(f0, f0, (int64_t)n, FE_FULL, c.s);
+    launch_fp12_mul(f0, f0, 1, dwp, 1, true, (int64_t)n, c.s);
+    launch_fp12_mul(dm, d3, 1, f0, 1, true, (int64_t)n, c.s);
     return c.finish();
 }
 
