@@ -248,3 +248,27 @@ def test_group_with_a_dishonest_party_matches_one_by_one():
     alone = [serving.decrypt_request(dk, cts, keys, ChaCha20Rng.seed_from_u64(5), cache) for cts in batches]
     assert grouped == alone
     assert all(r is not None for res in grouped for r in res)
+
+
+def test_graph_replayed_groups_match_the_direct_groups():
+    """The batched decryption captured once as a CUDA graph and replayed for
+    later groups of the same shape (new inputs copied into its buffers) gives
+    the direct call's messages, group after group; a committee or group size
+    it has not seen is captured on first use."""
+    rng = ChaCha20Rng.seed_from_u64(33)
+    mat = wb.keygen_with_rng(wb.KeygenConfig(8, [3, 2, 4, 1], 4), rng)
+    dk = mat.decryption_key
+    keys = [mat.party_keys[0], mat.party_keys[2]]
+    cache = serving.CommitteeCache(1 << 30)
+    graphs = serving.DecryptGraphs()
+    for k, K in enumerate((4, 4, 4, 2)):
+        msgs, batches = [], []
+        for _ in range(K):
+            m = wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(8)])
+            msgs.append(m)
+            batches.append(wb.encrypt_many(mat.encryption_key, m, rng))
+        direct = serving.decrypt_group(dk, batches, keys, ChaCha20Rng.seed_from_u64(k), cache)
+        replayed = serving.decrypt_group(dk, batches, keys, ChaCha20Rng.seed_from_u64(k), cache, graphs=graphs)
+        assert replayed == direct == msgs
+    assert graphs.captures == 2 and graphs.replays == 4
+    assert all(v > 10 for v in graphs.kernels.values())

@@ -188,6 +188,64 @@ class CommitteeCache:
         return len(self._entries)
 
 
+class DecryptGraphs:
+    """The batched decryption (wbte_wbtx_decrypt_many) replayed as captured
+    CUDA graphs.  For each prepared committee, batch size and group size, a
+    thread captures the call once into static device buffers; later groups of
+    the same shape copy their inputs in and replay the graph, which launches
+    the whole kernel sequence (transforms, Miller loops, final
+    exponentiations, products) as one unit.  The call has no host-synchronous
+    step when every buffer is on the device, so it captures as is; a warm-up
+    call first fills the library's caches (twiddles, occupancy queries)."""
+
+    def __init__(self):
+        self._local = threading.local()
+        self.captures = 0
+        self.replays = 0
+        self.kernels = {}  # shape -> kernels launched per replay
+
+    def run(self, pre: wb.DecryptionPrecomputation, first, second, valid, sigma_dev, T: int, B: int, K: int):
+        torch = wb._t()
+        table = getattr(self._local, "table", None)
+        if table is None:
+            table = self._local.table = {}
+        key = (pre.context_id, B, K, T)
+        ent = table.get(key)
+        if ent is None:
+            ent = table[key] = self._capture(pre, T, B, K)
+        ent["first"].copy_(first)
+        ent["second"].copy_(second)
+        ent["valid"].copy_(valid)
+        ent["sigma"].copy_(sigma_dev)
+        ent["graph"].replay()
+        self.replays += 1
+        return ent["out"].clone()
+
+    def _capture(self, pre, T, B, K):
+        torch = wb._t()
+        st = {"first": wb.empty_device(G1B * B * K), "second": wb.empty_device(GTB * B * K),
+              "valid": wb.empty_device(B * K), "sigma": wb.empty_device(G1B * T * K),
+              "out": wb.empty_device(GTB * B * K)}
+        for t in st.values():
+            t.zero_()
+
+        def call():
+            wb._ctx().call("wbte_wbtx_decrypt_many", st["out"], pre.kernel_lines, pre.opening_keys,
+                           pre.opening_lines, st["first"], st["second"], st["valid"], st["sigma"], T, B, K)
+
+        call()  # warm-up outside the capture
+        torch.cuda.current_stream().synchronize()
+        lib = _lib.load()
+        n0 = lib.wbte_ctx_launch_count(None)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            call()
+        self.kernels[(B, K, T)] = int(lib.wbte_ctx_launch_count(None) - n0)
+        self.captures += 1
+        st["graph"] = g
+        return st
+
+
 def decrypt_request(dk: wb.PublicDecryptionKey, ciphertexts, party_keys: Sequence[wb.PartySecretKey], rng,
                     cache: Optional[CommitteeCache] = None, device_output: bool = False):
     """One batch decryption: validate, committee partial decryptions, share
@@ -201,12 +259,14 @@ def decrypt_request(dk: wb.PublicDecryptionKey, ciphertexts, party_keys: Sequenc
 
 
 def decrypt_group(dk: wb.PublicDecryptionKey, batches: Sequence, party_keys: Sequence[wb.PartySecretKey], rng,
-                  cache: Optional[CommitteeCache] = None, device_output: bool = False) -> List:
+                  cache: Optional[CommitteeCache] = None, device_output: bool = False,
+                  graphs: Optional[DecryptGraphs] = None) -> List:
     """The batched form: K batches of one size, decrypted by one committee,
     with every GPU phase launched once for all K (the wbte_wbtx_*_many calls).
     Per batch the result is exactly `decrypt_request`'s: validation,
     transcripts, digests and the share-acceptance rules run per batch; a batch
-    whose aggregate share check fails falls back to the per-share path alone."""
+    whose aggregate share check fails falls back to the per-share path alone.
+    With `graphs`, the final decryption of each part is a replayed CUDA graph."""
     torch = wb._t()
     K = len(batches)
     if K == 0:
@@ -265,11 +325,14 @@ def decrypt_group(dk: wb.PublicDecryptionKey, batches: Sequence, party_keys: Seq
             f_p = torch.cat([first[G1B * B * b : G1B * B * (b + 1)] for b in idx])
             v_p = torch.cat([valid[B * b : B * (b + 1)] for b in idx])
             s_p = torch.cat([second_all[GTB * B * b : GTB * B * (b + 1)] for b in idx])
-        out = wb.empty_device(GTB * B * Kp)
         # precompute_batch and open_batch of the part's batches, the cross terms
         # and the opening pairings sharing one hard final exponentiation per slot
-        ctx.call("wbte_wbtx_decrypt_many", out, pre.kernel_lines, pre.opening_keys, pre.opening_lines, f_p, s_p,
-                 v_p, sigmas, Ta, B, Kp)
+        if graphs is not None:
+            out = graphs.run(pre, f_p, s_p, v_p, wb.to_device(sigmas), Ta, B, Kp)
+        else:
+            out = wb.empty_device(GTB * B * Kp)
+            ctx.call("wbte_wbtx_decrypt_many", out, pre.kernel_lines, pre.opening_keys, pre.opening_lines, f_p, s_p,
+                     v_p, sigmas, Ta, B, Kp)
         if device_output:
             for q, b in enumerate(idx):
                 results[b] = out[GTB * B * q : GTB * B * (q + 1)]
