@@ -415,6 +415,19 @@ def wpfe_section(args, torch, wb, flush, world, max_over_ranks, barrier):
             assert out[b] == msgs[b], "batched weighted_pfe decryption mismatch"
     barrier()
     wall = max_over_ranks(statistics.median(walls))
+    # per-kernel device time of one group of the largest class, alone on one stream
+    from weighted_bte_b200 import _lib
+
+    big = max(classes)
+    idx = [b for b, s in enumerate(sizes) if wpb.size_class(s) == big]
+    sc = classes[big]
+    _lib.profile_enable(True)
+    wpb.decrypt_group(sc.material.encryption_key, sc.material.decryption_key, [sc.pad(batches[b]) for b in idx],
+                      sc.party_keys, ChaCha20Rng.seed_from_u64(7), dec.cache, device_output=True)
+    torch.cuda.synchronize()
+    prof = _lib.profile_read()
+    _lib.profile_enable(False)
+    class_kernels = {k: round(v[0], 2) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
     real = sum(sizes)
     slots = sum(wpb.size_class(s) for s in sizes)
     per_class = {}
@@ -431,6 +444,7 @@ def wpfe_section(args, torch, wb, flush, world, max_over_ranks, barrier):
         "host plaintext lists out, classes on 4 CUDA streams, committees cached",
         "class_ms_summed": round(statistics.median(gpu_ms), 2), "classes": per_class,
         "keygen_s": round(keygen_s, 1), "warm_and_tune_s": round(tune_s, 1),
+        "largest_class_kernel_ms": {"class": big, "batches": len(idx), "kernels": class_kernels},
     }
 
 
