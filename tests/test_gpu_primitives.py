@@ -198,10 +198,12 @@ def test_gt_transforms_match_oracle(orc, n, lanes, monkeypatch):
     assert got == expect
 
 
-@pytest.mark.parametrize("count,lanes", [(32, "auto"), (32, "1"), (32, "2"), (33, "1"), (32, "4")])
+@pytest.mark.parametrize("count,lanes", [(32, "auto"), (32, "1"), (32, "2"), (33, "1"), (32, "4"), (27, "1"),
+                                         (27, "auto"), (20, "1")])
 def test_gt_transforms_many_match_oracle(orc, count, lanes, monkeypatch):
     """Batches of transforms in one launch per stage: 32 arrays give every
-    warp one twiddle power (the warp-uniform NAF plan), 33 arrays mix
+    warp one twiddle power (the warp-uniform NAF plan), 33 arrays run as 32
+    plus one, 27 arrays run the plan padded to 32 slots, 20 arrays mix
     twiddles within warps (the fixed schedule)."""
     if lanes != "auto":
         monkeypatch.setenv("WBTE_GT_LANES", lanes)

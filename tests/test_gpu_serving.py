@@ -272,3 +272,21 @@ def test_graph_replayed_groups_match_the_direct_groups():
         assert replayed == direct == msgs
     assert graphs.captures == 2 and graphs.replays == 4
     assert all(v > 10 for v in graphs.kernels.values())
+
+
+@pytest.mark.parametrize("K", [27, 37])
+def test_group_sizes_off_a_multiple_of_32_match_one_by_one(K):
+    """27 batches run the batched transforms padded to 32 slots, 37 batches as
+    32 plus a remainder of 5; both equal the batches decrypted one by one."""
+    rng = ChaCha20Rng.seed_from_u64(35 + K)
+    mat = wb.keygen_with_rng(wb.KeygenConfig(4, [3, 2, 4, 1], 4), rng)
+    dk = mat.decryption_key
+    keys = [mat.party_keys[0], mat.party_keys[2]]
+    msgs, batches = [], []
+    for _ in range(K):
+        m = wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(4)])
+        msgs.append(m)
+        batches.append(wb.encrypt_many(mat.encryption_key, m, rng))
+    cache = serving.CommitteeCache(1 << 30)
+    out = serving.decrypt_group(dk, batches, keys, ChaCha20Rng.seed_from_u64(3), cache)
+    assert out == msgs

@@ -431,10 +431,13 @@ static __device__ __noinline__ G1X g1_mul_joint_naf(const G1X v, const uint8_t* 
 // take the transforms fastest, so a warp shares one twiddle.
 template <class F>
 __global__ void __launch_bounds__(WARP) k_ntt_stage_joint(uint8_t* work, const uint8_t* tw, int64_t n, int64_t half,
-                                                         int64_t count) {
+                                                         int64_t count, int64_t pad) {
+    // threads take the transforms fastest over `pad` >= count slots; slots
+    // past count idle (pad a multiple of 32: every warp shares one twiddle)
     const int64_t g = (int64_t)blockIdx.x * WARP + threadIdx.x;
-    if (g >= (n / 2) * count) return;
-    const int64_t q = g % count, tt = g / count;
+    if (g >= (n / 2) * pad) return;
+    const int64_t q = g % pad, tt = g / pad;
+    if (q >= count) return;
     const int64_t chunk = tt / half, j = tt % half;
     const int64_t a = q * n + chunk * 2 * half + j, b = a + half;
     Xyzz<F>* w = reinterpret_cast<Xyzz<F>*>(work);
@@ -442,8 +445,8 @@ __global__ void __launch_bounds__(WARP) k_ntt_stage_joint(uint8_t* work, const u
     if (j != 0) {
         const uint8_t* sc = tw + FR_SZ * (j * (n / (2 * half)));
         if constexpr (std::is_same<F, Fp>::value) {
-            // whole warps share the twiddle when the transforms come in multiples of 32
-            t = count % WARP == 0 ? g1_mul_joint_naf(t, sc) : mul_joint(t, sc);
+            // whole warps share the twiddle when the slots come in multiples of 32
+            t = pad % WARP == 0 ? g1_mul_joint_naf(t, sc) : mul_joint(t, sc);
         } else {
             t = mul_joint(t, sc);
         }
@@ -1087,14 +1090,16 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
         note_launch();
         k_ntt_load<Fp><<<blocks_for(total), TPB, 0, s>>>(work, io, n, bits, count);
         const bool joint = ntt_joint(g, butterflies);
+        // 24..31 transforms run padded to 32 slots: warp-uniform NAF twiddles
+        // with at most a quarter of the lanes idle
+        const int64_t pad = count >= 24 && count < WARP ? (int64_t)WARP : count;
         for (int64_t half = 1; half < n; half *= 2) {
             note_launch();
             if (joint)
-                k_ntt_stage_joint<Fp><<<blocks_for(butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
+                k_ntt_stage_joint<Fp><<<blocks_for((n / 2) * pad, WARP), WARP, 0, s>>>(work, tw, n, half, count, pad);
             else
                 k_ntt_stage<Fp><<<blocks_for(NttLanes<Fp>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
         }
-        note_launch();
         launch_xyzz_to_affine(GROUP_G1, io, work, total, s);
     } else {
         note_launch();
@@ -1103,11 +1108,10 @@ void launch_group_ntt(Group g, uint8_t* io, uint8_t* work, const uint8_t* tw, in
         for (int64_t half = 1; half < n; half *= 2) {
             note_launch();
             if (joint)
-                k_ntt_stage_joint<Fp2><<<blocks_for(butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
+                k_ntt_stage_joint<Fp2><<<blocks_for(butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count, count);
             else
                 k_ntt_stage<Fp2><<<blocks_for(NttLanes<Fp2>::L * butterflies, WARP), WARP, 0, s>>>(work, tw, n, half, count);
         }
-        note_launch();
         launch_xyzz_to_affine(GROUP_G2, io, work, total, s);
     }
 }
