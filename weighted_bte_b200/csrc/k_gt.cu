@@ -327,6 +327,28 @@ __global__ void __launch_bounds__(WARP, WBTE_GT_MINBLOCKS) k_gt_pow(uint8_t* out
     if (active && c == 0) store_vec(as_gt(out) + i, load_vec(sh + lane));
 }
 
+// out[q B + i] = base[q B + i]^(scalars[i]) for K arrays of B values sharing
+// the B exponents (a slot's exponent is the same in every array): threads
+// take the arrays fastest over `pad` >= K slots (a multiple of 32), so every
+// warp shares one exponent and runs its width-4 NAF plan without divergence;
+// slots past K idle.
+__global__ void __launch_bounds__(WARP, WBTE_PLAN_MINBLOCKS) k_gt_pow_shared_plan(uint8_t* out, const uint8_t* base,
+                                                                                   const uint8_t* scalars, int64_t B,
+                                                                                   int64_t K, int64_t pad) {
+    const int64_t g = (int64_t)blockIdx.x * WARP + threadIdx.x;
+    if (g >= B * pad) return;
+    const int64_t q = g % pad, i = g / pad;
+    if (q >= K) return;
+    const Fp12 x = load_vec(as_gt(base) + q * B + i);
+    uint32_t sc[8];
+    load_scalar(sc, scalars + FR_SZ * i);
+    CycPlan pl;
+    make_cyc_plan(pl, sc);
+    Fp12 r;
+    cyc_pow_plan(r, x, pl);
+    store_vec(as_gt(out) + q * B + i, r);
+}
+
 // out[i] = base[i stride]^c_i for small signed c_i on cyclotomic values:
 // square-and-multiply over the bits of |c_i| with cyclotomic squarings, then
 // the inverse (conjugation) for negative c_i -- mul_cyclotomic_signed_small of
@@ -350,6 +372,16 @@ __global__ void k_gt_pow_small(uint8_t* out, const uint8_t* base, int64_t stride
 }
 
 }  // namespace
+
+bool launch_gt_pow_shared(uint8_t* out, const uint8_t* base, const uint8_t* scalars, int64_t B, int64_t K,
+                          cudaStream_t s) {
+    const int64_t pad = K % WARP == 0 ? K : (K >= 24 && K < WARP ? (int64_t)WARP : 0);
+    if (pad == 0 || B <= 0) return false;
+    ProfScope prof_("gt_pow", s);
+    note_launch();
+    k_gt_pow_shared_plan<<<blocks_for(B * pad, WARP), WARP, 0, s>>>(out, base, scalars, B, K, pad);
+    return true;
+}
 
 void launch_gt_pow_small(uint8_t* out, const uint8_t* base, int64_t stride, const int32_t* coeffs, int64_t n,
                          cudaStream_t s) {

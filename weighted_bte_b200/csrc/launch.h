@@ -158,6 +158,11 @@ void launch_cyclotomic_prefix_ifft(uint8_t* io, const uint8_t* twiddles_inv, int
 void launch_gt_ntt(uint8_t* io, const uint8_t* twiddles, int64_t n, cudaStream_t s, int64_t count = 1, bool inverse = false);
 // out[i] = base[i * stride]^scalars[i] on GT
 void launch_gt_pow(uint8_t* out, const uint8_t* base, int64_t base_stride, const uint8_t* scalars, int64_t n, cudaStream_t s);
+// out[q B + i] = base[q B + i]^scalars[i] for K arrays sharing B exponents, with
+// warp-uniform plans; returns false (launching nothing) when K is not 24..31
+// or a multiple of 32
+bool launch_gt_pow_shared(uint8_t* out, const uint8_t* base, const uint8_t* scalars, int64_t B, int64_t K,
+                          cudaStream_t s);
 // out[i] = base[i * stride]^coeffs[i] on cyclotomic values, small signed exponents
 void launch_gt_pow_small(uint8_t* out, const uint8_t* base, int64_t stride, const int32_t* coeffs, int64_t n,
                          cudaStream_t s);

@@ -1636,8 +1636,11 @@ static bool wpfe_open_core(Call& c, uint8_t* dm, const uint8_t* ds, uint64_t T, 
     launch_final_exp(mp, mp, (int64_t)n, FE_EASY, c.s);
     // mask = hard(mp / (ft pairing_cauchy)^(alpha (alpha + 1))); message = second / mask (:614-643)
     launch_fp12_mul(ft, ft, 1, dpc, 1, false, (int64_t)n, c.s);
-    launch_gather(apr, dap, dia, (int64_t)n, FR_SZ, c.s);
-    launch_gt_pow(f, ft, 1, apr, (int64_t)n, c.s);
+    // the slot's exponent is shared by the K batches: warp-uniform plans when K allows
+    if (!launch_gt_pow_shared(f, ft, dap, (int64_t)B, (int64_t)K, c.s)) {
+        launch_gather(apr, dap, dia, (int64_t)n, FR_SZ, c.s);
+        launch_gt_pow(f, ft, 1, apr, (int64_t)n, c.s);
+    }
     launch_fp12_mul(mp, mp, 1, f, 1, true, (int64_t)n, c.s);
     launch_final_exp(mp, mp, (int64_t)n, FE_HARD, c.s);
     launch_fp12_mul(dm, d2, 1, mp, 1, true, (int64_t)n, c.s);
