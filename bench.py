@@ -92,6 +92,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-wpfe", action="store_true", help="skip the batched weighted_pfe section")
     ap.add_argument("--no-sweep", action="store_true", help="skip the kernel sweep")
+    ap.add_argument("--no-plain", action="store_true", help="skip the one-batch-per-step arms (profiling runs)")
+    ap.add_argument("--no-graph", action="store_true", help="skip the graph-replayed batched arm")
     ap.add_argument("--wpfe-passes", type=int, default=2, help="timed passes over the 256 weighted_pfe batches")
     ap.add_argument("--no-served", action="store_true", help="skip the served weighted_pfe section")
     ap.add_argument("--served-requests", type=int, default=48, help="requests per pass of the served section")
@@ -716,12 +718,6 @@ def main():
     def step_cached(rb):
         return serving.decrypt_request(dk, rb, keys, ChaCha20Rng.seed_from_u64(99), cache, device_output=True)
 
-    # ---- plain: one batch per step on one stream, committee prepared every batch
-    for i in range(args.warmup):
-        out = step_plain(dev_p[i])
-    torch.cuda.synchronize()
-    if args.warmup:  # correctness gate (untimed)
-        assert wb.to_host(out, 576 * B) == b"".join(plain_p[args.warmup - 1])
     try:
         uuid = str(torch.cuda.get_device_properties(local).uuid)
         gpu_id = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
@@ -731,29 +727,40 @@ def main():
     barrier()
     torch.cuda.synchronize()
     sampler.start()
-    launches0 = _lib.load().wbte_ctx_launch_count(None)
-    _lib.profile_enable(True)
-    outs, ms_plain = timed_steps(torch, step_plain, dev_p[args.warmup:], flush, stream)
-    barrier()
-    prof = _lib.profile_read()
-    _lib.profile_enable(False)
-    launches_plain = _lib.load().wbte_ctx_launch_count(None) - launches0
-    for i in range(args.steps):
-        assert wb.to_host(outs[i], 576 * B) == b"".join(plain_p[args.warmup + i]), "decryption mismatch"
-    ms_plain = max_over_ranks(ms_plain)
-    plain_value = world * B * args.steps / (ms_plain / 1000.0)
+    plain_value = cached_value = ms_plain = ms_cached = None
+    launches_plain, prof = 0, {}
+    if not args.no_plain:
+        # ---- plain: one batch per step on one stream, committee prepared every batch
+        for i in range(args.warmup):
+            out = step_plain(dev_p[i])
+        torch.cuda.synchronize()
+        if args.warmup:  # correctness gate (untimed)
+            assert wb.to_host(out, 576 * B) == b"".join(plain_p[args.warmup - 1])
+        barrier()
+        torch.cuda.synchronize()
+        launches0 = _lib.load().wbte_ctx_launch_count(None)
+        _lib.profile_enable(True)
+        outs, ms_plain = timed_steps(torch, step_plain, dev_p[args.warmup:], flush, stream)
+        barrier()
+        prof = _lib.profile_read()
+        _lib.profile_enable(False)
+        launches_plain = _lib.load().wbte_ctx_launch_count(None) - launches0
+        for i in range(args.steps):
+            assert wb.to_host(outs[i], 576 * B) == b"".join(plain_p[args.warmup + i]), "decryption mismatch"
+        ms_plain = max_over_ranks(ms_plain)
+        plain_value = world * B * args.steps / (ms_plain / 1000.0)
 
-    # ---- plain_cached: one batch per step, committee preparation cached
-    for i in range(args.warmup):
-        out = step_cached(dev_p[i])
-    torch.cuda.synchronize()
-    barrier()
-    outs, ms_cached = timed_steps(torch, step_cached, dev_p[args.warmup:], flush, stream)
-    barrier()
-    for i in range(args.steps):
-        assert wb.to_host(outs[i], 576 * B) == b"".join(plain_p[args.warmup + i]), "decryption mismatch"
-    ms_cached = max_over_ranks(ms_cached)
-    cached_value = world * B * args.steps / (ms_cached / 1000.0)
+        # ---- plain_cached: one batch per step, committee preparation cached
+        for i in range(args.warmup):
+            out = step_cached(dev_p[i])
+        torch.cuda.synchronize()
+        barrier()
+        outs, ms_cached = timed_steps(torch, step_cached, dev_p[args.warmup:], flush, stream)
+        barrier()
+        for i in range(args.steps):
+            assert wb.to_host(outs[i], 576 * B) == b"".join(plain_p[args.warmup + i]), "decryption mismatch"
+        ms_cached = max_over_ranks(ms_cached)
+        cached_value = world * B * args.steps / (ms_cached / 1000.0)
 
     # ---- batched: each step runs C groups concurrently (one CUDA stream each);
     # a group is G batches with every GPU phase launched once over all of them
@@ -784,6 +791,8 @@ def main():
     # as a captured CUDA graph (one capture per stream thread and shape)
     batched_graph = None
     try:
+        if args.no_graph:
+            raise RuntimeError("skipped (--no-graph)")
         graphs = serving.DecryptGraphs()
 
         def step_graph(idx):
@@ -925,7 +934,7 @@ def main():
 
     # the plain path's dominant kernel: the preparation's G2 MSM segments
     top = max(prof.items(), key=lambda kv: kv[1][0]) if prof else ("none", (0.0, 0))
-    msm_g2_ms = prof.get("msm_segments_g2", (0.0, 0))[0] / args.steps
+    msm_g2_ms = prof.get("msm_segments_g2", (0.0, 0))[0] / args.steps if prof else None
     msm_g2_work = sum(wc.msm_expected(weights[j], B, True) for j in committee) + wc.msm_expected(W_T, B - 1, True)
     roofline_plain = roof("k_segments<Fp2> (committee preparation: B x T party-block G2 MSMs and B - 1 kernel "
                           "G2 MSMs of W_T terms per batch)", msm_g2_ms, msm_g2_work, peak,
@@ -966,13 +975,16 @@ def main():
                        f"CUDA stream each), {G} batches per group with every GPU phase launched once per group; "
                        f"committee preparation cached (the timed region's first group prepares)",
                        "l2": "flushed before every step (256 MB write)"},
-            "plain": {"value": plain_value, "unit": "ciphertexts/s", "ms_per_batch": ms_plain / args.steps,
+            "plain": {"value": plain_value, "unit": "ciphertexts/s",
+                      "ms_per_batch": ms_plain / args.steps if ms_plain else None,
                       "form": "one batch per step on one stream, committee prepared every batch (reference decrypt())",
                       "gpu_launches": int(launches_plain)},
-            "plain_cached": {"value": cached_value, "unit": "ciphertexts/s", "ms_per_batch": ms_cached / args.steps,
+            "plain_cached": {"value": cached_value, "unit": "ciphertexts/s",
+                             "ms_per_batch": ms_cached / args.steps if ms_cached else None,
                              "form": "one batch per step on one stream, committee preparation cached"},
-            "batched_over_plain": value / plain_value,
-            "batched_over_plain_cached": value / cached_value, "batched_graph": batched_graph,
+            "batched_over_plain": value / plain_value if plain_value else None,
+            "batched_over_plain_cached": value / cached_value if cached_value else None,
+            "batched_graph": batched_graph,
             "e2e": e2e, "gpu_launches": int(launches_b), "roofline": roofline, "rooflines": rooflines,
             "roofline_plain": roofline_plain, "cpu_baseline": cpu, "clocks": clocks,
             "kernel_ms_per_batch_plain": phases, "kernel_ms_per_group": group_kernels,
