@@ -902,14 +902,17 @@ def main():
                     peak_basis=peak_basis, batches_per_launch=G, dominant_in_group=top_g[0] == "gt_ifft",
                     work_basis="exact count of the Fp products the kernels run (warp-uniform NAF plans of the "
                                "twiddles, butterfly outputs); Fp additions not counted")
-    tr = traffic.get("k_gt_radix4_pows_plan")
-    if tr and ms_of.get("gt_ifft"):
-        # traffic of one plan launch scaled from the captured case by powers per launch
-        powers = 3 * (m // 4) * G
-        roofline["traffic"] = tr["dram_bytes_per_launch"] * powers / tr["powers_per_launch"]
+    tr = traffic.get("gt_ifft")
+    if tr and ms_of.get("gt_ifft") and tr.get("group") == G and tr.get("batch_size") == B:
+        # DRAM bytes of the phase's launches in one group, from the committed
+        # one-metric ncu capture of this configuration; the stack traffic does
+        # not grow in proportion to the group size, so no other size uses it
+        roofline["traffic"] = tr["dram_bytes_per_group"]
         roofline["traffic_basis"] = tr["basis"]
     else:
         roofline["traffic"] = None
+        roofline["traffic_basis"] = (f"no DRAM capture of this configuration (B = {B}, {G} batches per group) "
+                                     "in profiles/roofline_traffic.json")
     if ms_of.get("gt_ifft") and m == work["cyclotomic_prefix_ifft"]["m"]:
         oracle_count = G * work["cyclotomic_prefix_ifft"]["fp_products"]
         roofline["oracle_count_frac"] = oracle_count / (ms_of["gt_ifft"] / 1000.0) / peak
