@@ -918,13 +918,16 @@ def main():
         roofline["oracle_count_frac"] = oracle_count / (ms_of["gt_ifft"] / 1000.0) / peak
         roofline["oracle_count_basis"] = ("the oracle's count of the reference algorithm (radix-2, plain tower "
                                           "arithmetic): a side figure, not the kernel's work")
+    # run length of the share check's multi-Miller loops, from its profile tag
+    miller_run = next((int(k[len("miller_c"):]) for k in ms_of if k.startswith("miller_c")), 1)
     rooflines = {
         "miller_lines": roof("k_miller_lines (precompute: prepared Miller loops of the transformed first "
                              "components)", ms_of.get("miller_lines"), wc.MILLER_WITH_LINES * m * G, peak),
         "miller_lines_multi": roof("k_miller_lines_multi (opening: one multi-Miller loop of T pairings per slot)",
                                    ms_of.get("miller_lines_multi"), wc.multi_miller_with_lines(T) * B * G, peak),
-        "miller": roof("k_miller (share check: unprepared Miller loops of B + 1 pairs per batch)",
-                       ms_of.get("miller"), wc.MILLER_UNPREPARED * (B + 1) * G, peak),
+        "miller": roof(f"k_miller_chunks (share check: unprepared multi-Miller loops of B + 1 pairs per batch in "
+                       f"runs of {miller_run} pairs per thread)", ms_of.get(f"miller_c{miller_run}"),
+                       wc.multi_miller_unprepared(B + 1, miller_run) * G, peak),
         "final_exp_hard": roof("k_final_exp hard part (one per slot)", ms_of.get("final_exp_hard"),
                                wc.FINAL_EXP_HARD * B * G, peak),
         "ntt_g1": roof("k_ntt_stage_joint<Fp> (batched G1 transforms of the first components)",

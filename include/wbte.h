@@ -72,15 +72,20 @@ int32_t wbte_ctx_synchronize(wbte_ctx *ctx);
  *                          (0: cost model)
  *   WBTE_TUNE_NTT_JOINT    G1/G2 transform stages: 1 one thread per
  *                          butterfly, 0 the lane split (-1: cost model)
+ *   WBTE_TUNE_MILLER_CHUNK pairs per thread of the share checks' unprepared
+ *                          multi-Miller loops, 1..8 (0: cost model)
  * WBTE_ERR_INVALID_ARG for an unknown knob or a value out of range. */
 #define WBTE_TUNE_GT_LANES 1
 #define WBTE_TUNE_MSM_WINDOW 2
 #define WBTE_TUNE_MSM_SEGMENTS 3
 #define WBTE_TUNE_NTT_JOINT 4
+#define WBTE_TUNE_MILLER_CHUNK 5
 int32_t wbte_ctx_set_tuning(wbte_ctx *ctx, int32_t knob, int64_t value);
 const char *wbte_ctx_last_error(const wbte_ctx *ctx);
 /* Number of kernels the library has launched so far (all contexts). */
 uint64_t wbte_ctx_launch_count(const wbte_ctx *ctx);
+/* Kernels the library has launched from the calling thread so far. */
+uint64_t wbte_thread_launch_count(void);
 /* Per-kernel timing.  While enabled, every kernel launch is bracketed by CUDA
  * events on its stream; enabling (or disabling) clears the records.
  * wbte_profile_read synchronises the device and returns, per kernel name,

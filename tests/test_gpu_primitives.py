@@ -60,6 +60,27 @@ def test_g2_msm_matches_oracle(orc, n):
     assert ops.g2_msm(b"".join(points), sc) == orc.g2_msm(points, sc)
 
 
+@pytest.mark.parametrize("segments", [9, 31, 33, 64, 1000])
+def test_msm_segment_trees_match_oracle(orc, segments):
+    """Forced segment counts per window: the segment sums reduce by
+    warp-shuffle trees of 32 (full and ragged last trees) and by a final
+    per-thread sum, and the MSMs still equal the oracle's."""
+    from weighted_bte_b200 import _lib
+
+    rng = random.Random(300 + segments)
+    p1 = orc.g1_mul_many(orc.g1_generator(), rs(rng, 513, orc.R))
+    s1 = rs(rng, 513, orc.R)
+    p2 = orc.g2_mul_many(orc.g2_generator(), rs(rng, 150, orc.R))
+    s2 = rs(rng, 150, orc.R)
+    ctx = _lib.default_context(0)
+    ctx.set_tuning(_lib.TUNE_MSM_SEGMENTS, segments)
+    try:
+        assert ops.g1_msm(b"".join(p1), s1) == orc.g1_msm(p1, s1)
+        assert ops.g2_msm(b"".join(p2), s2) == orc.g2_msm(p2, s2)
+    finally:
+        ctx.set_tuning(_lib.TUNE_MSM_SEGMENTS, 0)
+
+
 def test_msm_family_indexed_and_vectors(orc, pts):
     g1, g2 = pts
     rng = random.Random(3)

@@ -162,6 +162,52 @@ def test_fixed_base_share_check_matches_pippenger():
         assert got["tables"] == got["pippenger"] == expect
 
 
+@pytest.mark.parametrize("chunk", [1, 2, 3, 8])
+def test_share_checks_with_chunked_miller_loops(chunk):
+    """The share checks' multi-Miller loops over runs of `chunk` pairs (9
+    pairs per batch: ragged last runs for 2 and 8, one run-length of 3, one
+    pair per thread for 1) accept honest shares and reject a tampered one,
+    in the batched and the single-batch check."""
+    from weighted_bte_b200 import _lib
+    from weighted_bte_b200.rng import sample_nonzero
+
+    rng = ChaCha20Rng.seed_from_u64(23)
+    mat = wb.keygen_with_rng(wb.KeygenConfig(8, [3, 2, 4, 1], 4), rng)
+    dk = mat.decryption_key
+    keys = [mat.party_keys[0], mat.party_keys[2], mat.party_keys[3]]
+    K, B, T = 3, 8, len(keys)
+    batches = []
+    for _ in range(K):
+        msgs = wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(B)])
+        batches.append(wb.validate_batch(dk, wb.encrypt_many(mat.encryption_key, msgs, rng)))
+    import torch
+
+    first = torch.cat([v.first_dev[: 96 * B] for v in batches])
+    shares = [wb.partial_decrypt_many(keys, v) for v in batches]
+    sig = b"".join(s.sigma for sh in shares for s in sh)
+    parties = [k.party_index for k in keys]
+    chal = [sample_nonzero(rng) for _ in range(K * T)]
+    ch = b"".join(wb.fr_bytes(x) for x in chal)
+    bad = bytearray(sig)
+    bad[96 * (2 * T + 1) + 7] ^= 0x04  # batch 2, second share
+    ctx = wb._ctx()
+    ctx.set_tuning(_lib.TUNE_MILLER_CHUNK, chunk)
+    try:
+        for s, expect in ((sig, [1, 1, 1]), (bytes(bad), [1, 1, 0])):
+            ok = np.zeros(K, dtype=np.int32)
+            ctx.call("wbte_wbtx_verify_shares_many", ok, dk.abi_key(), first, B, s, _lib.i64_array(parties), ch, T,
+                     K, None)
+            assert list(ok) == expect
+        for b in range(K):
+            assert wb._verify_shares(dk, batches[b], shares[b], chal[b * T : (b + 1) * T])
+        tampered = list(shares[2])
+        tampered[1] = wb.DecryptionShare(tampered[1].party_index, bytes(bad[96 * (2 * T + 1) : 96 * (2 * T + 2)]),
+                                         tampered[1].batch_digest, tampered[1].setup_id)
+        assert not wb._verify_shares(dk, batches[2], tampered, chal[2 * T : 3 * T])
+    finally:
+        ctx.set_tuning(_lib.TUNE_MILLER_CHUNK, 0)
+
+
 def test_fused_decryption_matches_precompute_then_open():
     """wbte_wbtx_decrypt_many (one hard final exponentiation per slot), with
     and without the opening keys' line tables, equals precompute_many
@@ -272,6 +318,54 @@ def test_graph_replayed_groups_match_the_direct_groups():
         assert replayed == direct == msgs
     assert graphs.captures == 2 and graphs.replays == 4
     assert all(v > 10 for v in graphs.kernels.values())
+
+
+def test_graph_captures_beside_concurrent_groups():
+    """Three threads on their own streams run grouped decryptions with graph
+    replay at once, so captures overlap other threads' uploads, validations
+    and launches (the batched form's layout); every group gives the direct
+    call's messages."""
+    import threading
+
+    import torch
+
+    rng = ChaCha20Rng.seed_from_u64(34)
+    mat = wb.keygen_with_rng(wb.KeygenConfig(8, [3, 2, 4, 1], 4), rng)
+    dk = mat.decryption_key
+    keys = [mat.party_keys[0], mat.party_keys[2]]
+    cache = serving.CommitteeCache(1 << 30)
+    graphs = serving.DecryptGraphs()
+    work = []
+    for _ in range(3):
+        groups = []
+        for _ in range(3):
+            msgs = [wb.messages_from_bytes([rng.fill_bytes(32) for _ in range(8)]) for _ in range(4)]
+            groups.append((msgs, [wb.encrypt_many(mat.encryption_key, m, rng) for m in msgs]))
+        work.append(groups)
+    direct = [[serving.decrypt_group(dk, b, keys, ChaCha20Rng.seed_from_u64(7), cache) for _, b in groups]
+              for groups in work]
+    got, errors = [None] * 3, []
+    device = torch.cuda.current_device()
+
+    def worker(w):
+        try:
+            torch.cuda.set_device(device)
+            with torch.cuda.stream(torch.cuda.Stream()):
+                got[w] = [serving.decrypt_group(dk, b, keys, ChaCha20Rng.seed_from_u64(7), cache, graphs=graphs)
+                          for _, b in work[w]]
+                torch.cuda.current_stream().synchronize()
+        except BaseException as exc:  # noqa: BLE001
+            errors.append(exc)
+
+    threads = [threading.Thread(target=worker, args=(w,)) for w in range(3)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for w in range(3):
+        assert got[w] == direct[w] == [m for m, _ in work[w]]
+    assert graphs.captures == 3 and graphs.replays == 9
 
 
 @pytest.mark.parametrize("K", [27, 37])

@@ -31,7 +31,7 @@ STATUS_NAMES = {
     -8: "WBTE_ERR_INTERNAL",
 }
 FE_FULL, FE_EASY, FE_HARD = 0, 1, 2
-TUNE_GT_LANES, TUNE_MSM_WINDOW, TUNE_MSM_SEGMENTS, TUNE_NTT_JOINT = 1, 2, 3, 4
+TUNE_GT_LANES, TUNE_MSM_WINDOW, TUNE_MSM_SEGMENTS, TUNE_NTT_JOINT, TUNE_MILLER_CHUNK = 1, 2, 3, 4, 5
 CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 G1_BYTES, G2_BYTES, GT_BYTES, FR_BYTES, LINE_BYTES, MILLER_LINES = 96, 192, 576, 32, 288, 68
 FIXED_TABLE_BYTES = 192 * 11 * 32  # fixed-base table of one G2 point (wbte_wbtx_vk_tables)
@@ -187,7 +187,8 @@ _SIGNATURES = {
 EXPORTED = sorted(
     list(_SIGNATURES)
     + ["wbte_version", "wbte_ctx_create", "wbte_ctx_destroy", "wbte_ctx_set_stream", "wbte_ctx_synchronize",
-       "wbte_ctx_last_error", "wbte_ctx_launch_count", "wbte_profile_enable", "wbte_profile_read",
+       "wbte_ctx_last_error", "wbte_ctx_launch_count", "wbte_thread_launch_count", "wbte_profile_enable",
+       "wbte_profile_read",
        "wbte_g1_msm_static", "wbte_ctx_set_tuning", "wbte_crs_upload_wbtx", "wbte_crs_upload_wpfe",
        "wbte_crs_destroy", "wbte_server_create", "wbte_submit", "wbte_poll", "wbte_server_destroy"]
 )
@@ -246,6 +247,8 @@ def load():
         lib.wbte_ctx_last_error.restype = ctypes.c_char_p
         lib.wbte_ctx_launch_count.argtypes = [_VP]
         lib.wbte_ctx_launch_count.restype = _U64
+        lib.wbte_thread_launch_count.argtypes = []
+        lib.wbte_thread_launch_count.restype = _U64
         lib.wbte_profile_enable.argtypes = [_I32]
         lib.wbte_profile_enable.restype = _I32
         lib.wbte_profile_read.argtypes = [_VP, _I32, _VP, _VP, _I32, ctypes.POINTER(_I32)]

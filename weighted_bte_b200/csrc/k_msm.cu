@@ -175,6 +175,35 @@ __global__ void k_reduce(uint8_t* out, const uint8_t* in, int64_t rows, int64_t 
     store_vec(reinterpret_cast<Xyzz<F>*>(out) + gid, acc);
 }
 
+// out[row * out_len + i] = sum of in[row * len + 32 i .. 32 i + 31]: one warp
+// per output, a shuffle tree of five additions (lanes past len hold the
+// identity); every lane runs each level, so the warp never diverges around
+// the shuffles.
+template <class F>
+__global__ void k_reduce_warp(uint8_t* out, const uint8_t* in, int64_t rows, int64_t len, int64_t out_len) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (wid >= rows * out_len) return;  // whole warps: rows * out_len warps are launched
+    const int64_t row = wid / out_len, i = wid % out_len, x = i * 32 + lane;
+    Xyzz<F> acc;
+    if (x < len) {
+        acc = load_vec(reinterpret_cast<const Xyzz<F>*>(in) + row * len + x);
+    } else {
+        set_inf(acc);
+    }
+    constexpr int WORDS = sizeof(Xyzz<F>) / 4;
+    for (int off = 16; off > 0; off >>= 1) {
+        Xyzz<F> other;
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&other);
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&acc);
+#pragma unroll
+        for (int w = 0; w < WORDS; w++) dst[w] = __shfl_down_sync(0xffffffffu, src[w], off);
+        if (lane + off >= 32) set_inf(other);
+        acc = xyzz_add(acc, other);
+    }
+    if (lane == 0) store_vec(reinterpret_cast<Xyzz<F>*>(out) + wid, acc);
+}
+
 template <class F>
 __global__ void k_combine(uint8_t* out, const uint8_t* wins, int64_t k, int windows, int c) {
     int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -245,11 +274,15 @@ void run_family(uint8_t* out, const uint8_t* points, const int64_t* pbase, const
     uint8_t* bufs[2] = {red, seg};
     int flip = 0;
     while (len > 1) {
-        int64_t G = len < 8 ? len : 8;
-        int64_t out_len = (len + G - 1) / G;
+        // long rows: warp-shuffle trees of 32; the last few per row: one thread
+        const int64_t G = len > 8 ? 32 : len;
+        const int64_t out_len = (len + G - 1) / G;
         uint8_t* dst = bufs[flip];
         note_launch();
-        k_reduce<F><<<blocks_for(rows * out_len, 64), 64, 0, s>>>(dst, src, rows, len, G, out_len);
+        if (G == 32)
+            k_reduce_warp<F><<<blocks_for(rows * out_len * 32, 64), 64, 0, s>>>(dst, src, rows, len, out_len);
+        else
+            k_reduce<F><<<blocks_for(rows * out_len, 64), 64, 0, s>>>(dst, src, rows, len, G, out_len);
         src = dst;
         flip ^= 1;
         len = out_len;

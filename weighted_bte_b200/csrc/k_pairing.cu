@@ -67,6 +67,26 @@ __global__ void WBTE_PAIR_BOUNDS k_miller(uint8_t* out, const uint8_t* p, const 
     store_vec(as_gt(out) + i, f);
 }
 
+// Segment s of `per` consecutive pairs is split into `chunks` runs of at most
+// C pairs; thread (s, ch) writes the product of its run's Miller loops, one
+// multi-Miller loop sharing the squarings.
+__global__ void WBTE_PAIR_BOUNDS k_miller_chunks(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t per,
+                                                 int64_t K, int C, int64_t chunks) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= K * chunks) return;
+    const int64_t s = g / chunks, lo = (g % chunks) * C;
+    const int cnt = (int)(per - lo < C ? per - lo : C);
+    G1A P[MULTI_MILLER_MAX];
+    G2A Q[MULTI_MILLER_MAX];
+    for (int t = 0; t < cnt; t++) {
+        P[t] = load_affine(reinterpret_cast<const G1A*>(p + G1_AFF * (s * per + lo + t)));
+        Q[t] = load_affine(reinterpret_cast<const G2A*>(q + G2_AFF * (s * per + lo + t)));
+    }
+    Fp12 f;
+    multi_miller_loop(f, P, Q, cnt);
+    store_vec(as_gt(out) + g, f);
+}
+
 __global__ void k_fp12_segment_product(uint8_t* out, const uint8_t* in, const int64_t* offsets, int64_t k) {
     int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= k) return;
@@ -233,6 +253,39 @@ void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, 
     if (n <= 0) return;
     note_launch();
     k_miller<<<blocks_for(n), TPB, 0, s>>>(out, p, q, n, p_mod, q_mod);
+}
+// Pairs per thread of the chunked unprepared Miller loops: sharing the 62
+// squarings over C pairs saves 2,232 Fp products per extra pair (about a
+// third of a loop), so chunks grow only while the launch keeps at least
+// half the resident threads busy (other streams fill the rest).
+int miller_chunk(int64_t pairs) {
+    if (g_tune.miller_chunk > 0) return g_tune.miller_chunk;
+    static std::atomic<int64_t> resident{0};
+    int64_t r = resident.load();
+    if (r == 0) {
+        int dev = 0, sms = 0, blocks = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_miller_chunks, TPB, 0);
+        r = (int64_t)(sms > 0 ? sms : 148) * (blocks > 0 ? blocks : 1) * TPB;
+        resident.store(r);
+    }
+    const int64_t C = 2 * pairs / r;
+    return (int)(C < 1 ? 1 : (C > MULTI_MILLER_MAX ? MULTI_MILLER_MAX : C));
+}
+int64_t launch_miller_chunks(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t per, int64_t K, int C,
+                             cudaStream_t s) {
+    if (per <= 0 || K <= 0) return 0;
+    if (C < 1) C = 1;
+    if (C > MULTI_MILLER_MAX) C = MULTI_MILLER_MAX;
+    // the profile tag names the run length, which fixes the product count
+    static const char* const tags[MULTI_MILLER_MAX + 1] = {"", "miller_c1", "miller_c2", "miller_c3", "miller_c4",
+                                                          "miller_c5", "miller_c6", "miller_c7", "miller_c8"};
+    ProfScope prof_(tags[C], s);
+    const int64_t chunks = (per + C - 1) / C;
+    note_launch();
+    k_miller_chunks<<<blocks_for(K * chunks), TPB, 0, s>>>(out, p, q, per, K, C, chunks);
+    return chunks;
 }
 void launch_fp12_mask(uint8_t* io, const uint8_t* valid, int64_t n, cudaStream_t s) {
     if (n <= 0) return;

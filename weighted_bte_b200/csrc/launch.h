@@ -13,7 +13,11 @@ namespace wbte {
 
 // kernels launched by this library since load
 extern std::atomic<uint64_t> g_launches;
-inline void note_launch(uint64_t k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+extern thread_local uint64_t t_launches;
+inline void note_launch(uint64_t k = 1) {
+    g_launches.fetch_add(k, std::memory_order_relaxed);
+    t_launches += k;
+}
 
 // Optional per-kernel timing: while profiling is enabled, a ProfScope records
 // CUDA events around the launches in its scope, tagged with a kernel name.
@@ -36,6 +40,7 @@ struct Tuning {
     int msm_window = 0;    // Pippenger window width c, 4..13
     int msm_segments = 0;  // sorted-term segments per (MSM, window), 1..1024
     int ntt_joint = -1;    // G1/G2 transform stages: 1 one thread per butterfly, 0 the lane split
+    int miller_chunk = 0;  // pairs per thread of the chunked unprepared Miller loops, 1..8
 };
 extern thread_local Tuning g_tune;
 
@@ -142,6 +147,12 @@ void launch_miller_lines(uint8_t* out, const uint8_t* lines, const uint8_t* p, i
                          int64_t lines_n = 0);
 // out[i] = Miller(p[p_mod ? i % p_mod : i], q[i])
 // pair i: P[p_mod ? i % p_mod : i], Q[q_mod ? i % q_mod : i]
+// K segments of `per` consecutive (P, Q) pairs: out[s * chunks + ch] is the
+// product of the Miller loops of run ch (at most C pairs) of segment s;
+// returns chunks = ceil(per / C).  miller_chunk picks C for `pairs` in all.
+int miller_chunk(int64_t pairs);
+int64_t launch_miller_chunks(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t per, int64_t K, int C,
+                             cudaStream_t s);
 void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, cudaStream_t s, int64_t p_mod = 0,
                    int64_t q_mod = 0);
 // io[i] = 1 where valid[i] == 0

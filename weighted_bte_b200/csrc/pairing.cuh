@@ -135,6 +135,36 @@ static __device__ __noinline__ void multi_miller_loop_lines(Fp12& f, const Line*
     fp12_conj(f, f);
 }
 
+// Product of C <= MULTI_MILLER_MAX Miller loops with lines computed on the
+// fly (unprepared_multi_miller_loop, weighted_btx/src/final_exponentiation.rs:
+// 229-274): pairs (P[t], Q[t]) share one accumulator, so the 62 Fp12
+// squarings are paid once for all C pairs; identities contribute 1.
+static __device__ __noinline__ void multi_miller_loop(Fp12& f, const G1A* P, const G2A* Q, int C) {
+    G2Proj T[MULTI_MILLER_MAX];
+    bool live[MULTI_MILLER_MAX];
+    for (int t = 0; t < C; t++) {
+        live[t] = !is_inf(P[t]) && !is_inf(Q[t]);
+        if (live[t]) T[t] = g2proj_from_affine(Q[t]);
+    }
+    f = fp12_one();
+    for (int i = 62; i >= 0; i--) {
+        if (i != 62) fp12_sqr(f, f);
+        for (int t = 0; t < C; t++) {
+            if (!live[t]) continue;
+            Line l = line_double(T[t]);
+            mul_by_line(f, l, P[t]);
+        }
+        if ((X_ABS >> i) & 1) {
+            for (int t = 0; t < C; t++) {
+                if (!live[t]) continue;
+                Line l = line_add(T[t], Q[t]);
+                mul_by_line(f, l, P[t]);
+            }
+        }
+    }
+    fp12_conj(f, f);
+}
+
 // ------------------------------------------------- final exponentiation
 // f^((p^6 - 1)(p^2 + 1))
 static __device__ __noinline__ void final_exp_easy(Fp12& r, const Fp12& f) {

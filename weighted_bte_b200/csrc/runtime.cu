@@ -17,6 +17,7 @@ using namespace wbte;
 
 namespace wbte {
 std::atomic<uint64_t> g_launches{0};
+thread_local uint64_t t_launches = 0;
 
 namespace {
 struct ProfRec {
@@ -407,6 +408,10 @@ int32_t wbte_ctx_set_tuning(wbte_ctx* ctx, int32_t knob, int64_t value) {
         if (value < -1 || value > 1) break;
         ctx->tune.ntt_joint = (int)value;
         return WBTE_OK;
+    case WBTE_TUNE_MILLER_CHUNK:
+        if (value < 0 || value > 8) break;
+        ctx->tune.miller_chunk = (int)value;
+        return WBTE_OK;
     default:
         break;
     }
@@ -431,6 +436,8 @@ uint64_t wbte_ctx_launch_count(const wbte_ctx* ctx) {
     (void)ctx;
     return g_launches.load();
 }
+
+uint64_t wbte_thread_launch_count(void) { return t_launches; }
 
 int32_t wbte_measure_imad_rate(wbte_ctx* ctx, double* imad_per_s) {
     if (!ctx || !imad_per_s) return WBTE_ERR_INVALID_ARG;
@@ -934,8 +941,8 @@ int32_t wbte_wbtx_verify_shares(wbte_ctx* ctx, int32_t* ok, const wbte_wbtx_key*
         launch_msm_family(GROUP_G2, Q, dvk, dvbase, dpidx, dch, nullptr, 1, nv, (int64_t)T, c.s);
     }
     cudaMemcpyAsync(Q + G2_AFF * nv, g2, G2_AFF, cudaMemcpyDeviceToDevice, c.s);
-    launch_miller(f, P, Q, nv + 1, c.s);
-    fp12_product(c, prod, f, nv + 1);
+    const int64_t runs = launch_miller_chunks(f, P, Q, nv + 1, 1, miller_chunk(nv + 1), c.s);
+    fp12_product(c, prod, f, runs);
     launch_final_exp(prod, prod, 1, FE_FULL, c.s);
     launch_fp12_is_one(flag, prod, 1, c.s);
     uint8_t h = 0;
@@ -1218,8 +1225,8 @@ int32_t wbte_btx_verify(wbte_ctx* ctx, int32_t* ok, const void* first, const uin
     }
     launch_negate(GROUP_G1, P + G1_AFF * nv, dsig, 1, c.s);
     cudaMemcpyAsync(Q + G2_AFF * nv, g2, G2_AFF, cudaMemcpyDeviceToDevice, c.s);
-    launch_miller(f, P, Q, nv + 1, c.s);
-    fp12_product(c, prod, f, nv + 1);
+    const int64_t runs = launch_miller_chunks(f, P, Q, nv + 1, 1, miller_chunk(nv + 1), c.s);
+    fp12_product(c, prod, f, runs);
     launch_final_exp(prod, prod, 1, FE_FULL, c.s);
     launch_fp12_is_one(flag, prod, 1, c.s);
     uint8_t h = 0;
@@ -2141,8 +2148,8 @@ int32_t wbte_wbtx_verify_shares_many(wbte_ctx* ctx, int32_t* ok, const wbte_wbtx
     if (!c.ok()) return c.finish();
     launch_gather(gcol, g2, dgidx, (int64_t)K, G2_AFF, c.s);
     cudaMemcpy2DAsync(Q + G2_AFF * B, G2_AFF * P1, gcol, G2_AFF, G2_AFF, K, cudaMemcpyDeviceToDevice, c.s);
-    launch_miller(f, P, Q, (int64_t)(P1 * K), c.s);
-    fp12_segments_product(c, prod, f, (int64_t)P1, (int64_t)K);
+    const int64_t runs = launch_miller_chunks(f, P, Q, (int64_t)P1, (int64_t)K, miller_chunk((int64_t)(P1 * K)), c.s);
+    fp12_segments_product(c, prod, f, runs, (int64_t)K);
     launch_final_exp(prod, prod, (int64_t)K, FE_FULL, c.s);
     launch_fp12_is_one(flags, prod, (int64_t)K, c.s);
     std::vector<uint8_t> h(K);

@@ -200,6 +200,7 @@ class DecryptGraphs:
 
     def __init__(self):
         self._local = threading.local()
+        self._lock = threading.Lock()
         self.captures = 0
         self.replays = 0
         self.kernels = {}  # shape -> kernels launched per replay
@@ -218,7 +219,8 @@ class DecryptGraphs:
         ent["valid"].copy_(valid)
         ent["sigma"].copy_(sigma_dev)
         ent["graph"].replay()
-        self.replays += 1
+        with self._lock:
+            self.replays += 1
         return ent["out"].clone()
 
     def _capture(self, pre, T, B, K):
@@ -236,12 +238,25 @@ class DecryptGraphs:
         call()  # warm-up outside the capture
         torch.cuda.current_stream().synchronize()
         lib = _lib.load()
-        n0 = lib.wbte_ctx_launch_count(None)
+        n0 = lib.wbte_thread_launch_count()
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            call()
-        self.kernels[(B, K, T)] = int(lib.wbte_ctx_launch_count(None) - n0)
-        self.captures += 1
+        # Thread-local capture on a side stream: other threads keep launching,
+        # copying and allocating on their own streams meanwhile.  (The
+        # torch.cuda.graph context synchronizes the device and empties the
+        # allocator cache first, which breaks another thread's capture.)
+        cur = torch.cuda.current_stream()
+        side = torch.cuda.Stream()
+        side.wait_stream(cur)
+        with torch.cuda.stream(side):
+            g.capture_begin(capture_error_mode="thread_local")
+            try:
+                call()
+            finally:
+                g.capture_end()
+        cur.wait_stream(side)
+        with self._lock:
+            self.kernels[(B, K, T)] = int(lib.wbte_thread_launch_count() - n0)
+            self.captures += 1
         st["graph"] = g
         return st
 

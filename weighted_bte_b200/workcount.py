@@ -31,6 +31,16 @@ MILLER_WITH_LINES = MILLER_SQUARINGS * FP12_SQR + MILLER_LINES * LINE_MUL  # 515
 MILLER_UNPREPARED = MILLER_WITH_LINES + 63 * LINE_DOUBLE + 5 * LINE_ADD  # 6727
 
 
+MILLER_SQUARING_RUN = MILLER_SQUARINGS * FP12_SQR  # 2232
+
+
+def multi_miller_unprepared(pairs: int, run: int) -> int:
+    """Share-check Miller loops of `pairs` pairs in runs of `run` pairs per
+    thread, each run one multi-Miller loop sharing the 62 squarings."""
+    runs = -(-pairs // run)
+    return runs * MILLER_SQUARING_RUN + pairs * (MILLER_UNPREPARED - MILLER_SQUARING_RUN)
+
+
 def multi_miller_with_lines(T: int) -> int:
     """One slot's multi-Miller loop over T prepared line tables."""
     return MILLER_SQUARINGS * FP12_SQR + T * MILLER_LINES * LINE_MUL
