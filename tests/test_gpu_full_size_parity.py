@@ -86,3 +86,52 @@ def test_weighted_btx_benchmark_shape_matches_oracle_stage_by_stage(orc):
     opened = wb.open_batch(pre, accepted, batch, cts, cross)
     expect = [mm if v else None for mm, v in zip(msgs, obatch["valid"])]
     assert opened == W.open_batch(opre, sig, obatch, octs, obeta) == expect
+
+
+def test_weighted_pfe_b512_matches_oracle_stage_by_stage(orc):
+    """weighted_pfe at B = 512 (the config-4 class of 512 slots), every stage
+    against the oracle: key material, encryption, validation, partial
+    decryptions, committee preparation, the Cauchy cross terms (compared
+    after the hard part, where they are canonical) and the opened messages."""
+    from oracle import wpfe_oracle as X
+    from weighted_bte_b200 import ops
+    from weighted_bte_b200 import weighted_pfe as wp
+
+    B, weights, t, seed = 512, [1, 3, 2, 4], 4, 6
+    mat = wp.keygen_with_rng(wp.KeygenConfig(B, weights, t), ChaCha20Rng.seed_from_u64(seed))
+    key = X.keygen(B, weights, t, ChaCha20Rng.seed_from_u64(seed))
+    dk = mat.decryption_key
+    assert dk.alpha_points() == key["alpha"] and dk.domain_points() == key["eval_domain"]
+    assert wb.to_host(dk.verification_keys) == key["vk"]
+    assert wb.to_host(dk.d1) == key["d1"] and wb.to_host(dk.d2) == key["d2"]
+    assert dk.setup_id() == key["setup_id"]
+
+    msgs = ops.split(ops.gt_pow(wb.gt_generator(), [11 + i for i in range(B)], fixed_base=True), 576)
+    cts = wp.encrypt_many(mat.encryption_key, msgs, ChaCha20Rng.seed_from_u64(seed + 100))
+    octs = X.encrypt_many(key, msgs, ChaCha20Rng.seed_from_u64(seed + 100))
+    assert [dict(first=c.first, second=c.second, commitment=c.proof.commitment, response=c.proof.response)
+            for c in cts] == octs
+    batch = wp.validate_batch(mat.encryption_key, cts)
+    obatch = X.validate(key, octs)
+    assert batch.digest() == obatch["digest"]
+
+    shares = wp.partial_decrypt_many(mat.party_keys, batch)
+    assert [s.sigma for s in shares] == [X.partial_decrypt(key, j, obatch) for j in range(len(weights))]
+    accepted = wp.accept_decryption_shares(dk, batch, shares, ChaCha20Rng.seed_from_u64(1))
+    parties = accepted.party_indices()
+    assert parties == X.select_committee(key, range(len(weights)))
+    pre = wp.prepare_decryption(dk, accepted)
+    opre = X.prepare(key, parties)
+    assert wb.to_host(pre.scaled_d1_by_party) == b"".join(opre["by_party"])
+    assert wb.to_host(pre.scaled_d1_total) == b"".join(opre["total"])
+    assert wb.to_host(pre.mask_keys) == b"".join(opre["mask"])
+
+    kern = wp.CauchyKernel.new(dk)
+    bp = wp.precompute_batch(kern, pre, batch)
+    obp = X.precompute(key, opre, obatch)
+    assert wb.to_host(bp.scaled_first_cauchy, 96 * B) == b"".join(obp["first_cauchy"])
+    got_pc = ops.split(ops.final_exp(wb.to_host(bp.pairing_cauchy, 576 * B), mode=2), 576)
+    assert got_pc == orc.hard_final_exp_many(obp["pairing_cauchy"])
+
+    out = wp.open_batch(dk, kern, pre, accepted, batch, cts, bp)
+    assert out == X.open_batch(key, opre, [shares[j].sigma for j in parties], obatch, octs, obp) == msgs

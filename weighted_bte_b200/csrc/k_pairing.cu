@@ -256,8 +256,9 @@ void launch_miller(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t n, 
 }
 // Pairs per thread of the chunked unprepared Miller loops: sharing the 62
 // squarings over C pairs saves 2,232 Fp products per extra pair (about a
-// third of a loop), so chunks grow only while the launch keeps at least
-// half the resident threads busy (other streams fill the rest).
+// third of a loop), but a launch of fewer threads than the device holds
+// takes as long as the longest thread, so chunks grow only while the launch
+// still fills the resident threads.
 int miller_chunk(int64_t pairs) {
     if (g_tune.miller_chunk > 0) return g_tune.miller_chunk;
     static std::atomic<int64_t> resident{0};
@@ -270,7 +271,7 @@ int miller_chunk(int64_t pairs) {
         r = (int64_t)(sms > 0 ? sms : 148) * (blocks > 0 ? blocks : 1) * TPB;
         resident.store(r);
     }
-    const int64_t C = 2 * pairs / r;
+    const int64_t C = pairs / r;
     return (int)(C < 1 ? 1 : (C > MULTI_MILLER_MAX ? MULTI_MILLER_MAX : C));
 }
 int64_t launch_miller_chunks(uint8_t* out, const uint8_t* p, const uint8_t* q, int64_t per, int64_t K, int C,
