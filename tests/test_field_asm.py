@@ -47,10 +47,23 @@ class Machine:
         return self.reg[tok]
 
     def run(self, instrs):
-        for ins in instrs:
-            if ins.startswith(".reg"):
+        labels = {ins[:-1]: k for k, ins in enumerate(instrs) if ins.endswith(":")}
+        pc, steps = 0, 0
+        while pc < len(instrs):
+            ins = instrs[pc]
+            pc += 1
+            steps += 1
+            assert steps < 100000, "runaway loop"
+            if ins.startswith(".reg") or ins.endswith(":"):
                 continue
+            if ins.startswith("@"):
+                guard, ins = ins.split(None, 1)
+                if not self.reg[guard[1:]]:
+                    continue
             op, rest = ins.rstrip(";").split(None, 1)
+            if op == "bra":
+                pc = labels[rest.strip()]
+                continue
             args = [a.strip() for a in rest.split(",")]
             parts = op.split(".")
             base = parts[0]
@@ -81,8 +94,8 @@ class Machine:
             elif base == "and":
                 self.reg[args[0]] = self.val(args[1]) & self.val(args[2])
             elif base == "setp":
-                assert parts[1] == "eq"
-                self.reg[args[0]] = self.val(args[1]) == self.val(args[2])
+                x, y = self.val(args[1]), self.val(args[2])
+                self.reg[args[0]] = {"eq": x == y, "lt": x < y, "ne": x != y}[parts[1]]
             elif base == "selp":
                 self.reg[args[0]] = self.val(args[1]) if self.reg[args[3]] else self.val(args[2])
             else:
@@ -115,7 +128,8 @@ def edge_values(m):
     return [0, 1, 2, m - 1, m - 2, (m - 1) // 2, 1 << 255 if m > 1 << 256 else 1 << 200, m >> 1]
 
 
-@pytest.mark.parametrize("name,modulus,n", [("fp_mont_mul", P, 12), ("fr_mont_mul", R, 8)])
+@pytest.mark.parametrize("name,modulus,n", [("fp_mont_mul", P, 12), ("fp_mont_mul_r4", P, 12),
+                                            ("fp_mont_mul_r6", P, 12), ("fr_mont_mul", R, 8)])
 def test_montgomery_product(name, modulus, n):
     rng = random.Random(1)
     rinv = pow(1 << (32 * n), -1, modulus)

@@ -91,6 +91,92 @@ def gen_mont_mul(name, modulus, n):
     )
 
 
+def gen_mont_mul_rolled(name, modulus, n, unroll):
+    """The CIOS product of gen_mont_mul as a loop of n / unroll iterations of
+    `unroll` rows each (about a third of the code of the straight-line
+    sequence for unroll = 4, at the cost of the register rotation between
+    iterations).  Emitted for the code-size experiments of fetch-bound
+    kernels; one instance per translation unit (the loop label is fixed)."""
+    assert n % unroll == 0
+    pinv = (-pow(modulus, -1, 1 << 32)) % (1 << 32)
+    ml = limbs32(modulus, n)
+    lines = []
+    w = lines.append
+    w(".reg .u32 t<%d>, bb<%d>, m, bw, d<%d>, cnt, tmp;" % (n + 2, n, n))
+    w(".reg .pred nb, more;")
+    a = ["%%%d" % (n + i) for i in range(n)]
+    b = ["%%%d" % (2 * n + i) for i in range(n)]
+    out = ["%%%d" % i for i in range(n)]
+    canon = ["t%d" % i for i in range(n + 2)]
+    for i in range(n + 1):
+        w("mov.u32 %s, 0;" % canon[i])
+    for i in range(n):
+        w("mov.u32 bb%d, %s;" % (i, b[i]))
+    w("mov.u32 cnt, 0;")
+    w("$Lcios_%s:" % name)
+    t = list(canon)
+    for r in range(unroll):
+        bi = "bb%d" % r
+        w("mad.lo.cc.u32 %s, %s, %s, %s;" % (t[0], a[0], bi, t[0]))
+        for j in range(1, n):
+            w("madc.lo.cc.u32 %s, %s, %s, %s;" % (t[j], a[j], bi, t[j]))
+        w("addc.cc.u32 %s, %s, 0;" % (t[n], t[n]))
+        w("addc.u32 %s, 0, 0;" % t[n + 1])
+        w("mad.hi.cc.u32 %s, %s, %s, %s;" % (t[1], a[0], bi, t[1]))
+        for j in range(1, n):
+            w("madc.hi.cc.u32 %s, %s, %s, %s;" % (t[j + 1], a[j], bi, t[j + 1]))
+        w("addc.u32 %s, %s, 0;" % (t[n + 1], t[n + 1]))
+        w("mul.lo.u32 m, %s, 0x%08x;" % (t[0], pinv))
+        w("mad.lo.cc.u32 %s, m, 0x%08x, %s;" % (t[0], ml[0], t[0]))
+        for j in range(1, n):
+            w("madc.lo.cc.u32 %s, m, 0x%08x, %s;" % (t[j], ml[j], t[j]))
+        w("addc.cc.u32 %s, %s, 0;" % (t[n], t[n]))
+        w("addc.u32 %s, %s, 0;" % (t[n + 1], t[n + 1]))
+        w("mad.hi.cc.u32 %s, m, 0x%08x, %s;" % (t[1], ml[0], t[1]))
+        for j in range(1, n):
+            w("madc.hi.cc.u32 %s, m, 0x%08x, %s;" % (t[j + 1], ml[j], t[j + 1]))
+        w("addc.u32 %s, %s, 0;" % (t[n + 1], t[n + 1]))
+        t = t[1:] + [t[0]]
+    # back to the canonical names: canon[k] <- t[k] for all n + 2 registers,
+    # k -> k + unroll (mod n + 2) being a permutation, moved cycle by cycle
+    src = {canon[k]: t[k] for k in range(n + 2)}
+    done = set()
+    for start in canon:
+        if start in done or src[start] == start:
+            continue
+        chain = [start]
+        cur = src[start]
+        while cur != start:
+            chain.append(cur)
+            cur = src[cur]
+        w("mov.u32 tmp, %s;" % chain[0])
+        for k in range(len(chain) - 1):
+            w("mov.u32 %s, %s;" % (chain[k], chain[k + 1]))
+        w("mov.u32 %s, tmp;" % chain[-1])
+        done.update(chain)
+    for k in range(n - unroll):
+        w("mov.u32 bb%d, bb%d;" % (k, k + unroll))
+    w("add.u32 cnt, cnt, %d;" % unroll)
+    w("setp.lt.u32 more, cnt, %d;" % n)
+    w("@more bra $Lcios_%s;" % name)
+    t = list(canon)
+    w("sub.cc.u32 d0, %s, 0x%08x;" % (t[0], ml[0]))
+    for j in range(1, n):
+        w("subc.cc.u32 d%d, %s, 0x%08x;" % (j, t[j], ml[j]))
+    w("subc.cc.u32 bw, %s, 0;" % t[n])
+    w("subc.u32 bw, 0, 0;")
+    w("setp.eq.u32 nb, bw, 0;")
+    for j in range(n):
+        w("selp.u32 %s, d%d, %s, nb;" % (out[j], j, t[j]))
+    body = "\n".join("        \"" + l + "\\n\\t\"" for l in lines)
+    outs = ", ".join('"=r"(r[%d])' % i for i in range(n))
+    ins = ", ".join(['"r"(a[%d])' % i for i in range(n)] + ['"r"(b[%d])' % i for i in range(n)])
+    return (
+        "__device__ __forceinline__ void %s(uint32_t r[%d], const uint32_t a[%d], const uint32_t b[%d]) {\n"
+        "    asm(\"{\\n\\t\"\n%s\n        \"}\"\n        : %s\n        : %s);\n}\n" % (name, n, n, n, body, outs, ins)
+    )
+
+
 def gen_add(name, modulus, n):
     """r = a + b mod m (inputs < m)."""
     ml = limbs32(modulus, n)
@@ -463,6 +549,8 @@ def main():
         gen_sub("fp_sub_raw", P, 12),
         gen_add_nr("fp_add_nored", 12),
         gen_fp2_mul_lazy("fp2_mont_mul_lazy"),
+        gen_mont_mul_rolled("fp_mont_mul_r4", P, 12, 4),
+        gen_mont_mul_rolled("fp_mont_mul_r6", P, 12, 6),
         gen_mont_mul("fr_mont_mul", R, 8),
         gen_add("fr_add_raw", R, 8),
         gen_sub("fr_sub_raw", R, 8),
