@@ -41,7 +41,17 @@ SOURCE_UNDEFINES: dict = {"k_pairing.cu": ["WBTE_FP2_NOINLINE"]}
 # instruction fetch, keep the Fp2 product out of line and take the Fp sums
 # out of line too (the batched truncated transform of 64 batches: 140 ->
 # 124 ms; the same layout slows the Miller and final-exponentiation kernels).
-SOURCE_DEFINES: dict = {"k_gt.cu": ["WBTE_FPADD_NOINLINE"]}
+# The fetch-bound tower kernels also take the Fp product as a rolled loop of
+# rows (WBTE_FP_ROLLED rows per iteration: a third to a half of the code of
+# the straight-line product for about 10 % more instructions).  Measured on
+# B200 at 128 batches of B = 512 per group: the GT transform 246 -> 185 ms
+# (4 rows), the opening multi-Miller loops 72.7 -> 65.4 ms (6 rows), the hard
+# parts 47.3 -> 44.9 ms and the easy parts 13.8 -> 12.7 ms (4 rows); the curve
+# kernels (MSMs, G1 transforms, fixed-base tables) measured 2-7 % slower and
+# keep the straight-line product.
+SOURCE_DEFINES: dict = {"k_gt.cu": ["WBTE_FPADD_NOINLINE", "WBTE_FP_ROLLED=4"],
+                        "k_pairing.cu": ["WBTE_FP_ROLLED=4"],
+                        "k_opening.cu": ["WBTE_FP_ROLLED=6"]}
 
 
 def nvcc() -> str:
