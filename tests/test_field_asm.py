@@ -128,8 +128,7 @@ def edge_values(m):
     return [0, 1, 2, m - 1, m - 2, (m - 1) // 2, 1 << 255 if m > 1 << 256 else 1 << 200, m >> 1]
 
 
-@pytest.mark.parametrize("name,modulus,n", [("fp_mont_mul", P, 12), ("fp_mont_mul_r2", P, 12),
-                                            ("fp_mont_mul_r3", P, 12), ("fp_mont_mul_r4", P, 12),
+@pytest.mark.parametrize("name,modulus,n", [("fp_mont_mul", P, 12), ("fp_mont_mul_r4", P, 12),
                                             ("fp_mont_mul_r6", P, 12), ("fr_mont_mul", R, 8)])
 def test_montgomery_product(name, modulus, n):
     rng = random.Random(1)

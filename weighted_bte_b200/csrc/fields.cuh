@@ -27,13 +27,9 @@ WBTE_INL Fp fp_one() { Fp r; _Pragma("unroll") for (int i = 0; i < 12; i++) r.v[
 #if defined(WBTE_FP_NOINLINE)
 // One out-of-line copy of the 12-limb product keeps every kernel's hot loop
 // inside the instruction cache.
-#if defined(WBTE_FP_ROLLED) && WBTE_FP_ROLLED == 2
-// the same product as a loop of rows, `WBTE_FP_ROLLED` rows per iteration:
+#if defined(WBTE_FP_ROLLED) && WBTE_FP_ROLLED == 4
+// the same product as a loop of rows, WBTE_FP_ROLLED rows per iteration:
 // less code per product for kernels bound by instruction fetch
-static __device__ __noinline__ Fp fp_mul_ool(Fp a, Fp b) { Fp r; fp_mont_mul_r2(r.v, a.v, b.v); return r; }
-#elif defined(WBTE_FP_ROLLED) && WBTE_FP_ROLLED == 3
-static __device__ __noinline__ Fp fp_mul_ool(Fp a, Fp b) { Fp r; fp_mont_mul_r3(r.v, a.v, b.v); return r; }
-#elif defined(WBTE_FP_ROLLED) && WBTE_FP_ROLLED == 4
 static __device__ __noinline__ Fp fp_mul_ool(Fp a, Fp b) { Fp r; fp_mont_mul_r4(r.v, a.v, b.v); return r; }
 #elif defined(WBTE_FP_ROLLED) && WBTE_FP_ROLLED == 6
 static __device__ __noinline__ Fp fp_mul_ool(Fp a, Fp b) { Fp r; fp_mont_mul_r6(r.v, a.v, b.v); return r; }

@@ -549,8 +549,6 @@ def main():
         gen_sub("fp_sub_raw", P, 12),
         gen_add_nr("fp_add_nored", 12),
         gen_fp2_mul_lazy("fp2_mont_mul_lazy"),
-        gen_mont_mul_rolled("fp_mont_mul_r2", P, 12, 2),
-        gen_mont_mul_rolled("fp_mont_mul_r3", P, 12, 3),
         gen_mont_mul_rolled("fp_mont_mul_r4", P, 12, 4),
         gen_mont_mul_rolled("fp_mont_mul_r6", P, 12, 6),
         gen_mont_mul("fr_mont_mul", R, 8),
